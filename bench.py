@@ -1,0 +1,332 @@
+#!/usr/bin/env python
+"""vectors/s of the multi-grid PIV engine on one 6600x4400 image pair.
+
+Workload (one step = one image pair through the whole pipeline): 6600x4400 uint8 pair,
+MHE (40 px tiles, 0.91), grid 1 64x64 windows at 32 px spacing for 2 passes, grid 2
+32x32 at 16 px for 3 passes, window deformation, bilinear upsampling, normalized
+median test (5x5, 2 passes, threshold 2), hole fill, 3x3 smoothing, Nsec_cc = 1.
+Synthetic seeded particle images (0.04 particles/px, sigma 0.6 px, Lamb-Oseen vortex
+of 10 px peak speed and 600 px core radius plus 0.002 px/px shear).  Final vectors per
+pair: 113,300 (412 x 275).
+
+  value  device-resident: frames already in HBM, CUDA events on the engine stream around
+         each replay of the captured pair graph; L2 flushed before every step.
+  e2e    through the C-ABI with host buffers: upload of both frames from pinned memory,
+         the pair, readback of the filtered grid-2 field, every step.
+  --impl reference  the reference's own engine (xcorr2d_multi + mhe_gpu, compiled for
+         sm_100a from its sources) on the same pair through its public methods.
+
+Multi-GPU: one process per GPU; every rank processes its own pair (replicas, no data
+collective); torch.distributed only for the barrier and the max-over-ranks time.
+"""
+import argparse
+import importlib.util
+import json
+import math
+import os
+import re
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+PKG_DIR = ROOT / "piv_xcorr2d_v1.0_b200"
+sys.path.insert(0, str(ROOT))
+
+NX, NY = 6600, 4400
+METRIC = "vectors/s at 6600x4400 multigrid (64->32 px, 2+3 passes, MHE on)"
+UNIT = "vectors/s"
+
+
+def load_pkg():
+    if "piv_b200" in sys.modules:
+        return sys.modules["piv_b200"]
+    spec = importlib.util.spec_from_file_location("piv_b200", PKG_DIR / "__init__.py",
+                                                  submodule_search_locations=[str(PKG_DIR)])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["piv_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def workload_params(P, device_id=0, Ny=NY):
+    return P.default_params(device_id=device_id, Nx=NX, Ny=Ny, if_mhe=1, mhe_ws=40, mhe_thresh=0.91,
+                            ws_x1=64, ws_y1=64, spacing_x1=32, spacing_y1=32, Npass1=2,
+                            ws_x2=32, ws_y2=32, spacing_x2=16, spacing_y2=16, Npass2=3, Nsec_cc=1,
+                            insert_threshold_p1=2.0, insert_threshold_p2=2.0)
+
+
+def workload_pair(P, seed=1):
+    s = P.synth_params(NX, NY, ppp=0.04, sigma=0.6, field=P.PIV_FIELD_VORTEX, a=10.0, b=600.0, c=0.002, seed=seed)
+    return P.synth_pair(s)
+
+
+def fft_flops(wsx, wsy):
+    """Algorithmic FP32 flops of one window correlation: 3 transforms (5 N log2 N) + 8 N."""
+    n = wsx * wsy
+    return 3 * 5 * n * math.log2(n) + 8 * n
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while running."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.gpu), "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.out = ""
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                self.out, _ = self.proc.communicate()
+
+    def summary(self):
+        rows = []
+        for line in (self.out or "").splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                rows.append((float(f[1]), float(f[2]), f[5:9]))
+            except ValueError:
+                continue
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for _, _, r in rows for i, v in enumerate(r) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows),
+                "reasons": reasons, "samples": len(rows)}
+
+
+def traffic_from_profile():
+    """DRAM bytes per launch of the grid-2 correlation kernel from the committed ncu summary."""
+    f = ROOT / "profiles" / "xcorr_grid2_6600x4400.txt"
+    if not f.exists():
+        return None
+    m = re.search(r"dram_bytes_per_launch_full_size:\s*([0-9.eE+]+)", f.read_text())
+    return float(m.group(1)) if m else None
+
+
+def cpu_baseline(P, f1, f2, rows):
+    """The CPU oracle on a bounded band of the same pair (full pipeline), vectors/s."""
+    from oracle import oracle as O
+
+    p = workload_params(P, Ny=rows)
+    a = np.ascontiguousarray(f1[:rows])
+    b = np.ascontiguousarray(f2[:rows])
+    t0 = time.perf_counter()
+    a = O.mhe(a, 40, 0.91)
+    b = O.mhe(b, 40, 0.91)
+    r = O.run_pair(a, b, p)
+    dt = time.perf_counter() - t0
+    nvec = r["geom"]["Nt_vec"][1]
+    return {"value": nvec / dt, "unit": UNIT, "cores": O.threads(), "kind": "port",
+            "sample": f"CPU oracle (FP64 correlation) on the top {NX}x{rows} band of the pair, full pipeline "
+                      f"({nvec} grid-2 vectors in {dt:.2f} s)"}
+
+
+def dist_setup(n_gpus):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    return rank, world, local
+
+
+def dist_max(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def dist_barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def run_ours(args, rank, world, local):
+    import torch
+
+    P = load_pkg()
+    torch.cuda.set_device(local)
+    p = workload_params(P, device_id=local)
+    f1, f2 = workload_pair(P, seed=1 + rank)
+    d1 = torch.from_numpy(f1).to(f"cuda:{local}")
+    d2 = torch.from_numpy(f2).to(f"cuda:{local}")
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device=f"cuda:{local}")  # > 126 MB L2
+    e = P.Engine(p)
+    nvec = e.geom["Nt_vec"][1]
+    ext = torch.cuda.ExternalStream(e.stream(), device=f"cuda:{local}")
+    e.set_device_images(d1.data_ptr(), d2.data_ptr())
+    for _ in range(args.warmup):
+        e.run_pair()
+        e.synchronize()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    dist_barrier(world)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        for k in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            starts[k].record(ext)
+            e.run_pair()
+            ends[k].record(ext)
+        e.synchronize()
+        torch.cuda.synchronize()
+    dist_barrier(world)
+    ms = [starts[k].elapsed_time(ends[k]) for k in range(args.steps)]
+    total_s = dist_max(sum(ms) / 1e3, world)
+    value = world * args.steps * nvec / total_s
+
+    # end to end through the C-ABI with host buffers
+    h1, h2 = e.host_images()
+    h1[:] = f1
+    h2[:] = f2
+    e.set_device_images(0, 0)
+    e.run_pair()
+    e.field(3)
+    dist_barrier(world)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        e.run_pair()
+        _, _, dx, dy, vv = e.field(3)
+    e2e_s = dist_max(time.perf_counter() - t0, world)
+    e2e = {"value": world * args.steps * nvec / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 2 * NX * NY,
+           "d2h_bytes_per_step": int(dx.nbytes + dy.nbytes + vv.nbytes)}
+
+    # live roofline of the dominant kernel (grid-2 correlation), on the engine stream
+    e.set_device_images(d1.data_ptr(), d2.data_ptr())
+    e.run_pair()
+    e.synchronize()
+    kms = e.time_stage(1, reps=10)
+    flops = nvec * fft_flops(p.ws_x2, p.ws_y2)
+    peak = P.fp32_peak_tflops()
+    achieved = flops / (kms * 1e-3) / 1e12
+    roofline = {"bound": "fp32", "achieved": round(achieved, 2), "peak": round(peak, 2), "unit": "TFLOP/s",
+                "frac": round(achieved / peak, 4), "traffic": traffic_from_profile(),
+                "kernel": "xcorr_peak_kernel<32,32> (grid-2 correlation, deformed)",
+                "kernel_ms": round(kms, 4), "algorithmic_flops_per_launch": flops,
+                "peak_source": "FP32 FMA peak measured live on this GPU by piv_probe_fp32_peak"}
+    launches = e.launches_per_pair() * args.steps
+    out = {
+        "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(total_s * 1e3 / args.steps, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded particle images, Lamb-Oseen vortex + shear)",
+        "config": {"workload": "6600x4400 pair, MHE 40/0.91, grid 64x64@32 x2 -> 32x32@16 x3",
+                   "vectors_per_pair": nvec, "pairs_per_step_per_gpu": 1, "parallelism": f"replicas x{world}",
+                   "l2": "flushed (512 MB write) before every timed step"},
+        "e2e": e2e, "roofline": roofline, "gpu_launches": launches, "clocks": clk.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(P, f1, f2, args.cpu_rows)
+    e.close()
+    return out
+
+
+def run_reference(args, rank, world, local):
+    if rank != 0:
+        return None
+    P = load_pkg()
+    from oracle import ref as R
+
+    if not R.available():
+        return {"impl": "reference", "unavailable": "oracle/_ref/libref_xcorr2d.so was not built"}
+    p = workload_params(P, device_id=local)
+    f1, f2 = workload_pair(P, seed=1)
+    geom = P.geometry(p)
+    nvec = geom["Nt_vec"][1]
+    with R.RefEngine(p) as r:
+        for _ in range(args.warmup):
+            r.run_pair(f1, f2)
+            r.filtered(1, nvec)
+        with ClockSampler(local) as clk:
+            t0 = time.perf_counter()
+            for _ in range(args.steps):
+                r.run_pair(f1, f2)  # synchronises the device before returning
+                r.filtered(1, nvec)
+            dt = time.perf_counter() - t0
+    value = args.steps * nvec / dt
+    return {
+        "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(dt * 1e3 / args.steps, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "impl": "reference",
+        "data": "synthetic (seeded particle images, Lamb-Oseen vortex + shear)",
+        "config": {"workload": "6600x4400 pair, MHE 40/0.91, grid 64x64@32 x2 -> 32x32@16 x3",
+                   "vectors_per_pair": nvec, "pairs_per_step_per_gpu": 1, "parallelism": "replicas x1"},
+        "cpu_baseline": {"value": round(value, 1), "unit": UNIT, "cores": 1, "kind": "reference",
+                         "sample": "the reference's CUDA engine compiled for sm_100a from its own sources, driven "
+                                   "from one host thread through xcorr2d_multi/mhe_gpu in main.cpp order "
+                                   "(pinned host frames in, filtered grid-2 field out, wall clock)"},
+        "e2e": {"value": round(value, 1), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "clocks": clk.summary(),
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-rows", type=int, default=1024, help="rows of the pair the CPU baseline processes")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        # rank 0 alone runs the reference; the other ranks exit without work
+        rank = int(os.environ.get("RANK", "0"))
+        out = run_reference(args, rank, 1, int(os.environ.get("LOCAL_RANK", "0")))
+        if out is not None:
+            print(json.dumps(out))
+        return
+    rank, world, local = dist_setup(args.gpus)
+    out = run_ours(args, rank, world, local)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0 and out is not None:
+        print(json.dumps(out))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,281 @@
+/*
+ * piv_b200.h -- C-ABI of the B200-native multi-grid PIV correlation engine.
+ *
+ * A drop-in for the engine surface of xinzhixue/PIV_xcorr2d_V1.0 (paths below are
+ * relative to that project; X/ = xcorr2d_V1.0/):
+ *   class xcorr2d_multi  X/xcorr2d_multi_grid.cuh:12-208
+ *   class mhe_gpu        X/MHE7_4_gpu.h:7-40
+ * driven in the order of X/main.cpp:248-380.  Every entry point returns an int
+ * status (PIV_OK = 0, negative = error); piv_last_error() gives the message the
+ * reference would have printed.  One host thread per engine; calls on one engine
+ * are not re-entrant.  All device work is queued on the engine's own CUDA stream.
+ * Plain pointers and sizes only: no CUDA or C++ types cross this boundary.
+ */
+#ifndef PIV_B200_H
+#define PIV_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PIV_B200_ABI_VERSION 1
+
+/* Status codes. */
+#define PIV_OK 0
+#define PIV_ERR_ARG (-1)          /* invalid argument or parameter value */
+#define PIV_ERR_GEOMETRY (-2)     /* rejected by the window-size checks of xcorr2d_multi::init */
+#define PIV_ERR_UNSUPPORTED (-3)  /* valid for the reference but not built into this engine */
+#define PIV_ERR_CUDA (-4)         /* a CUDA runtime call failed */
+#define PIV_ERR_ALLOC (-5)        /* device or pinned allocation failed */
+#define PIV_ERR_IO (-6)           /* file could not be opened / parsed */
+#define PIV_ERR_STATE (-7)        /* call out of order (e.g. a pass before piv_prep) */
+#define PIV_ERR_DEVICE (-8)       /* a kernel reported an error status (iteration cap hit) */
+
+typedef struct piv_engine piv_engine;
+typedef struct piv_mhe piv_mhe;
+
+/* Numeric lines 7..50 of the reference's 50-line parameter file, in file order
+ * (X/main.cpp:103-146, X/Parameter_Instructions_xcorr2d_V1.0.txt:38-136). */
+typedef struct piv_params {
+    int device_id;                 /* 7  */
+    int if_mhe;                    /* 8  */
+    int mhe_ws;                    /* 9  */
+    float mhe_thresh;              /* 10 */
+    int Nx, Ny;                    /* 11, 12 */
+    int ws_x1, ws_y1;              /* 13, 14 */
+    int spacing_x1, spacing_y1;    /* 15, 16 */
+    int Npass1;                    /* 17 */
+    int ws_x2, ws_y2;              /* 18, 19 */
+    int spacing_x2, spacing_y2;    /* 20, 21 */
+    int Npass2;                    /* 22 */
+    int Nsec_cc;                   /* 23 */
+    int wx1_median, wy1_median;    /* 24, 25 */
+    int Npass1_median;             /* 26 */
+    int minNneigh_p1;              /* 27 */
+    float residual_threshold_p1;   /* 28 (read, unused: as in the reference) */
+    float insert_threshold_p1;     /* 29 */
+    int wx1_smooth, wy1_smooth;    /* 30, 31 */
+    int Npass1_smooth;             /* 32 */
+    int wx2_median, wy2_median;    /* 33, 34 */
+    int Npass2_median;             /* 35 */
+    int minNneigh_p2;              /* 36 */
+    float residual_threshold_p2;   /* 37 (read, unused) */
+    float insert_threshold_p2;     /* 38 */
+    int wx2_smooth, wy2_smooth;    /* 39, 40 */
+    int Npass2_smooth;             /* 41 */
+    float max_dispx_win_percent1;  /* 42 */
+    float max_dispy_win_percent1;  /* 43 */
+    float max_dispx_win_percent2;  /* 44 */
+    float max_dispy_win_percent2;  /* 45 */
+    int Npeak_save;                /* 46 */
+    float dispx_lim1, dispx_lim2;  /* 47, 48 */
+    float dispy_lim1, dispy_lim2;  /* 49, 50 */
+} piv_params;
+
+/* Lines 1..6 of the parameter file (file-name prefixes/suffixes, pair list, output folder). */
+typedef struct piv_paths {
+    char prefix_f1[1024], suffix_f1[256];
+    char prefix_f2[1024], suffix_f2[256];
+    char dir_index[1024];
+    char folder_result[1024];
+} piv_paths;
+
+/* Derived geometry, bit-identical to xcorr2d_multi::init (X/xcorr2d_multi_grid.cu:751-894). */
+typedef struct piv_geometry {
+    int border_x[2], border_y[2];
+    int hfws_x[2], hfws_y[2];
+    int Npeak[2];
+    int Nx_vec[2], Ny_vec[2], Nt_vec[2];
+    int Neach[2], Nlast[2], Nsec[2];
+    int Nx_left[2], Nx_right[2], Ny_left[2], Ny_right[2];
+    int Nx_aug[2], Ny_aug[2], Nx_aug_ex[2], Ny_aug_ex[2];
+} piv_geometry;
+
+/* ---- parameter file, geometry ------------------------------------------------ */
+
+/* Parses the 50-line positional parameter file (X/main.cpp:93-158).  Returns
+ * PIV_ERR_IO if it cannot be opened and PIV_ERR_ARG if a line is missing
+ * ("Parameter missing in Parameter.dat!").  paths may be NULL. */
+int piv_params_read(const char *path, piv_params *out, piv_paths *paths);
+
+/* Geometry without allocating an engine (same checks as xcorr2d_multi::init). */
+int piv_geometry_compute(const piv_params *p, piv_geometry *out);
+
+/* Message for a status code without an engine handle. */
+const char *piv_status_string(int status);
+
+/* ---- engine: xcorr2d_multi + mhe_gpu --------------------------------------- */
+
+/* mhe_gpu::init + xcorr2d_multi::init (X/MHE7_4_gpu.cu:149, X/xcorr2d_multi_grid.cu:716):
+ * selects p->device_id, validates the geometry, allocates all device buffers and
+ * the pinned host frame buffers, creates the engine stream. */
+int piv_create(const piv_params *p, piv_engine **out);
+
+/* xcorr2d_multi::freemem + mhe_gpu::freemem. */
+int piv_destroy(piv_engine *e);
+
+/* Message of the last failing call on this engine (empty if none). */
+const char *piv_last_error(const piv_engine *e);
+
+int piv_get_geometry(const piv_engine *e, piv_geometry *out);
+
+/* The parameters the engine was created with. */
+int piv_get_params(const piv_engine *e, piv_params *out);
+
+/* Engine-owned pinned host frame buffers, Nx*Ny bytes each, row-major without
+ * padding (the public h_img1_org / h_img2_org, X/xcorr2d_multi_grid.cuh:104-105). */
+int piv_host_images(piv_engine *e, uint8_t **f1, uint8_t **f2);
+
+/* Copies two host frames (Nx*Ny bytes each, rows of `pitch` bytes; pitch 0 = Nx)
+ * into the engine's pinned buffers. */
+int piv_set_images(piv_engine *e, const uint8_t *f1, const uint8_t *f2, size_t pitch);
+
+/* Uses two frames already resident in device memory (Nx*Ny bytes each, row-major)
+ * instead of the pinned host buffers for the next piv_prep. The pointers must stay
+ * valid until piv_prep has run. NULL, NULL switches back to the host buffers. */
+int piv_set_device_images(piv_engine *e, const uint8_t *d_f1, const uint8_t *d_f2);
+
+/* prep_img_data (X/xcorr2d_multi_grid.cu:1271-1282) fused with the optional MHE of
+ * both frames (X/main.cpp:267-283, mhe_gpu::processsing): uploads the frames (one
+ * asynchronous copy per frame from the pinned buffers, or a device-to-device copy),
+ * enhances them on the device when if_mhe == 1 and places them into the padded
+ * frame buffers.  No host round trip. */
+int piv_prep(piv_engine *e);
+
+/* Calc_cc_map_p1(idx_pass) (X/xcorr2d_multi_grid.cu:1284-1449), including the
+ * extend_filtered_vecfield_p1 that precedes it for idx_pass > 0. */
+int piv_pass_grid1(piv_engine *e, int idx_pass);
+
+/* MedianFilter_Smoothing_p1 (X/xcorr2d_multi_grid.cu:1451-1545). */
+int piv_validate_grid1(piv_engine *e, int Npass_median, int minNneigh, float residual_threshold,
+                       float insert_threshold, int Npass_smooth);
+
+/* extend_filtered_vecfield_p1 + Upsampling_vector_field (X/xcorr2d_multi_grid.cu:1547-1587). */
+int piv_upsample(piv_engine *e);
+
+/* extend_filtered_vecfield_p2 + Calc_cc_map_p2 (X/xcorr2d_multi_grid.cu:1589-1764). */
+int piv_pass_grid2(piv_engine *e);
+
+/* MedianFilter_Smoothing_p2 (X/xcorr2d_multi_grid.cu:1766-1863). */
+int piv_validate_grid2(piv_engine *e, int Npass_median, int minNneigh, float residual_threshold,
+                       float insert_threshold, int Npass_smooth, int iffill);
+
+/* The per-pair body of X/main.cpp:288-326 with the engine's parameters: prep (+MHE),
+ * the grid-1 passes and validations, upsampling, the grid-2 passes and validations.
+ * Replayed from a CUDA graph captured on the first call.  Asynchronous: follow with
+ * piv_synchronize or a piv_get_* call. */
+int piv_run_pair(piv_engine *e);
+
+/* Waits for the engine stream and reports any device-side error status. */
+int piv_synchronize(piv_engine *e);
+
+/* Field readback (synchronises).  selection as write_vec_data_general:
+ *   0 grid-1 raw candidates, 1 grid-1 filtered, 2 grid-2 raw candidates, 3 grid-2 filtered.
+ * For raw selections dx, dy, valid hold Nt_vec*Npeak_save values (candidate-major per
+ * vector); for filtered ones Nt_vec.  x, y receive the grid coordinates (Nt_vec).
+ * Any output pointer may be NULL. */
+int piv_get_field(piv_engine *e, int selection, float *x, float *y, float *dx, float *dy, uint8_t *valid);
+
+/* write_vec_data_general (X/xcorr2d_multi_grid.cu:1865-1973): Tecplot ASCII file. */
+int piv_write_tecplot(piv_engine *e, const char *path, int selection);
+
+/* The Tecplot writer on caller arrays (raw != 0: dx, dy hold Nt_vec*Npeak_save values and
+ * four candidate columns are printed, as the reference always does). */
+int piv_tecplot_write_arrays(const char *path, int Nx_vec, int Ny_vec, int spacing_x, int spacing_y, int raw,
+                             int Npeak_save, const float *dx, const float *dy);
+
+/* Output file name of X/main.cpp:327-369 for pair index `idx`:
+ * kind 0 grid-1 raw, 1 grid-1 filtered, 2 grid-2 raw, 3 grid-2 filtered, 4 grid-2 median-only. */
+int piv_output_name(const piv_params *p, const char *folder, int idx, int kind, char *out, size_t cap);
+
+/* ---- parity / diagnostics taps ---------------------------------------------- */
+
+/* Peak bookkeeping of the last pass of a grid: local-maximum count per vector
+ * (d_posi_count), chosen peak index in the shifted window (j*ws_x+i, -1 = none) and
+ * value, Npeak_save per vector.  Any pointer may be NULL. */
+int piv_get_peaks(piv_engine *e, int grid, int32_t *count, int32_t *peak_index, float *peak_value);
+
+/* Replaces the filtered field of a grid (the predictor of the next pass). */
+int piv_set_field(piv_engine *e, int grid, const float *dx, const float *dy, const uint8_t *valid);
+
+/* Replaces the raw candidates of a grid (input of the next validation). */
+int piv_set_candidates(piv_engine *e, int grid, const float *dx, const float *dy, const uint8_t *valid);
+
+/* Frames as placed by piv_prep (after MHE), Nx*Ny each. */
+int piv_get_frames(piv_engine *e, uint8_t *f1, uint8_t *f2);
+
+/* Deformed frame 2 of the last pass of a grid, [Ny_aug][Nx_aug] floats. */
+int piv_get_deformed(piv_engine *e, int grid, float *out);
+
+/* Re-runs the correlation of the last pass of `grid` for windows [first, first+n) and
+ * returns their shifted correlation planes ([n][ws_y][ws_x] floats); the candidates of
+ * those windows are rewritten with identical values. */
+int piv_debug_cc_planes(piv_engine *e, int grid, int first, int n, float *out);
+
+/* Device time of the kernels of the last piv_run_pair, by stage (ms): [0] prep+MHE,
+ * [1] deformation, [2] correlation, [3] validation, [4] total. Needs PIV_TIMING=1 in the
+ * environment at piv_create; otherwise returns PIV_ERR_STATE. */
+int piv_stage_times(piv_engine *e, float *ms5);
+
+/* ---- measurement ------------------------------------------------------------ */
+
+/* The engine's CUDA stream (a cudaStream_t), for callers that order their own work
+ * (events, copies) against the engine. */
+int piv_get_stream(const piv_engine *e, void **stream);
+
+/* Kernels that one piv_run_pair launches with the engine's parameters. */
+int piv_kernel_launches_per_pair(const piv_engine *e, int *n);
+
+/* Re-launches one stage `reps` times on the engine stream on the current state (the
+ * stage is idempotent on its inputs) and returns the mean device time per launch from
+ * CUDA events on that stream.  which: 0 grid-1 correlation kernel (last pass's mode),
+ * 1 grid-2 correlation kernel, 2 grid-2 deformation, 3 grid-2 validation (median passes
+ * + fill + smoothing with the engine's parameters), 4 MHE of one frame. */
+int piv_time_stage(piv_engine *e, int which, int reps, float *ms_per_launch);
+
+/* Measured FP32 FMA throughput of the current device (TFLOP/s, 2 flops per FMA), from a
+ * dependent-chain FMA kernel over every SM; the SIMT roofline of the FP32 correlation path. */
+int piv_probe_fp32_peak(float *tflops);
+
+/* ---- standalone MHE (mhe_gpu) --------------------------------------------- */
+
+/* mhe_gpu::init (X/MHE7_4_gpu.cu:149-212) on the current device. */
+int piv_mhe_create(int Nx, int Ny, int ws, float thresh, piv_mhe **out);
+/* mhe_gpu::processsing (X/MHE7_4_gpu.cu:214-253): d_in -> d_out, both Nx*Ny device bytes;
+ * pixels outside the centred crop are written 0.  stream: a cudaStream_t or NULL. */
+int piv_mhe_process(piv_mhe *m, const uint8_t *d_in, uint8_t *d_out, void *stream);
+int piv_mhe_destroy(piv_mhe *m);
+
+/* ---- synthetic particle-image pairs (no reference counterpart) -------------- */
+
+/* Displacement field models. */
+#define PIV_FIELD_UNIFORM 0   /* (a, b) */
+#define PIV_FIELD_VORTEX 1    /* Lamb-Oseen vortex: peak speed a, core radius b, plus shear c*(y-Ny/2) in x */
+#define PIV_FIELD_FOURIER 2   /* sum of 8 seeded Fourier modes, wavelengths in [a, b] px, max |u| c */
+
+typedef struct piv_synth_params {
+    int Nx, Ny;
+    double ppp;            /* particles per pixel */
+    double sigma;          /* Gaussian spot sigma, px */
+    double i_min, i_max;   /* peak intensity U(i_min, i_max) */
+    double background;     /* additive background */
+    double noise_sigma;    /* additive Gaussian noise sigma */
+    int field;             /* PIV_FIELD_* */
+    double a, b, c;        /* field parameters */
+    uint64_t seed;
+} piv_synth_params;
+
+/* Renders frame 1 (particles at x) and frame 2 (particles at x + u(x)) as uint8, Nx*Ny
+ * each; deterministic for a given seed (Philox4x32-10 counter RNG).  Host-only. */
+int piv_synth_pair(const piv_synth_params *s, uint8_t *f1, uint8_t *f2);
+
+/* The displacement field of s evaluated at n points. */
+int piv_synth_field(const piv_synth_params *s, const float *x, const float *y, int n, float *u, float *v);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

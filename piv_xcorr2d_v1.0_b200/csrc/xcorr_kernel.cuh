@@ -1,0 +1,345 @@
+// xcorr_kernel.cu -- the fused correlation + peak kernel (FP32 SIMT path).
+//
+// One launch replaces, for a section of windows, the reference's
+//   organize_data_fft2d_multi(_deformed)  X/xcorr2d_multi_grid.cu:497, 654
+//   cufftExecC2C FORWARD x2               :1334-1341, 1649-1656
+//   multiply_conjugate                    :519
+//   cufftExecC2C INVERSE                  :1347, 1662
+//   complex2amp_xcorr2d                   :536
+//   fftshift2d_xcorr2d_row/col            :547, 566
+//   find_local_max_2d                     :585
+//   reduce_max_index_general/final x4     :32, 103
+//   replace_local_max_2d                  :298
+//   peak_subpixel_4peak_2d                :309
+//   kernel_remove_nan                     :457
+// The correlation planes never leave shared memory.
+//
+// Per CTA: a batch of B windows (B even).  Data flow in shared memory:
+//   P1  row task (window, row): gather frame-1 and frame-2 rows straight from HBM,
+//       pack z = f1 + i*f2, row FFT in registers, store.
+//   P2  column task: column FFT in registers -> Z = FFT2(f1) + i*FFT2(f2).
+//   P3  column task (window pair, column): the cross spectrum conj(F1)*F2 follows
+//       from Z(k) and Z(-k) as  C = Im(Z(k)Z(-k))/2 + i(|Z(-k)|^2 - |Z(k)|^2)/4;
+//       it is Hermitian, so two windows share one inverse transform:
+//       W = C_a + i*C_b, inverse column FFT in registers.
+//   P4  row task (pair, row): inverse row FFT -> Re = corr_a, Im = corr_b;
+//       |.|/N written as fftshifted FP32 planes.
+//   P5  warp per window: 4-neighbour local maxima inside the search region,
+//       count, register top-K (value desc, then lower index), 3-point Gaussian fit
+//       with an FP64 log-ratio denominator, predictor, limits, NaN/Inf removal.
+#pragma once
+#include <cfloat>
+#include <climits>
+
+#include "fft_reg.cuh"
+#include "piv_common.cuh"
+
+namespace piv {
+
+template <int WSX>
+__device__ __forceinline__ void load_u8_row(const uint8_t *p, float (&v)[WSX])
+{
+    uintptr_t ad = reinterpret_cast<uintptr_t>(p);
+    if constexpr (WSX % 8 == 0) {
+        if ((ad & 7) == 0) {
+#pragma unroll
+            for (int q = 0; q < WSX / 8; ++q) {
+                uint2 u = __ldg(reinterpret_cast<const uint2 *>(p) + q);
+#pragma unroll
+                for (int b = 0; b < 4; ++b) {
+                    v[8 * q + b] = (float)((u.x >> (8 * b)) & 0xffu);
+                    v[8 * q + 4 + b] = (float)((u.y >> (8 * b)) & 0xffu);
+                }
+            }
+            return;
+        }
+    }
+    if ((ad & 3) == 0) {
+#pragma unroll
+        for (int q = 0; q < WSX / 4; ++q) {
+            uint32_t u = __ldg(reinterpret_cast<const uint32_t *>(p) + q);
+#pragma unroll
+            for (int b = 0; b < 4; ++b) v[4 * q + b] = (float)((u >> (8 * b)) & 0xffu);
+        }
+        return;
+    }
+#pragma unroll
+    for (int i = 0; i < WSX; ++i) v[i] = (float)__ldg(p + i);
+}
+
+template <int WSX>
+__device__ __forceinline__ void load_f32_row(const float *p, float (&v)[WSX])
+{
+    if ((reinterpret_cast<uintptr_t>(p) & 15) == 0) {
+#pragma unroll
+        for (int q = 0; q < WSX / 4; ++q) {
+            float4 u = __ldg(reinterpret_cast<const float4 *>(p) + q);
+            v[4 * q] = u.x;
+            v[4 * q + 1] = u.y;
+            v[4 * q + 2] = u.z;
+            v[4 * q + 3] = u.w;
+        }
+        return;
+    }
+#pragma unroll
+    for (int i = 0; i < WSX; ++i) v[i] = __ldg(p + i);
+}
+
+// total order used for the top-K: larger value first, then the lower index
+__device__ __forceinline__ bool better(float v1, int i1, float v2, int i2)
+{
+    return v1 > v2 || (v1 == v2 && i1 < i2);
+}
+
+template <int K>
+__device__ __forceinline__ void topk_insert(float (&tv)[K], int (&ti)[K], float v, int i)
+{
+    if (!better(v, i, tv[K - 1], ti[K - 1])) return;
+#pragma unroll
+    for (int s = K - 1; s >= 1; --s) {
+        bool up = better(v, i, tv[s - 1], ti[s - 1]);  // v goes above slot s-1
+        bool here = !up && better(v, i, tv[s], ti[s]);
+        float nv = up ? tv[s - 1] : (here ? v : tv[s]);
+        int ni = up ? ti[s - 1] : (here ? i : ti[s]);
+        tv[s] = nv;
+        ti[s] = ni;
+    }
+    if (better(v, i, tv[0], ti[0])) {
+        tv[0] = v;
+        ti[0] = i;
+    }
+}
+
+template <int WSX, int WSY, int B, int NT, int K, bool DEF>
+__global__ void __launch_bounds__(NT) xcorr_peak_kernel(const XcorrArgs a)
+{
+    static_assert(B % 2 == 0, "windows are processed in pairs");
+    constexpr int LDX = WSX + 1;   // complex row stride (odd -> conflict-free rows and columns)
+    constexpr int WIN = WSY * LDX; // complex elements per window buffer
+    constexpr int LDF = WSX + 1;   // float row stride of the correlation planes
+    constexpr float inv_n = 1.0f / (float)(WSX * WSY);
+    extern __shared__ float2 sm[];
+
+    const GridGeom &g = a.g;
+    const int tid = threadIdx.x;
+    const int w_base = a.w_first + blockIdx.x * B;
+
+    // ---------------- P1: row gather + forward row FFT ----------------
+    for (int t = tid; t < B * WSY; t += NT) {
+        const int b = t / WSY, r = t - b * WSY;
+        const int w = w_base + b;
+        float2 z[WSX];
+        if (w < a.w_end) {
+            const int iy = w / g.Nx_vec, ix = w - iy * g.Nx_vec;
+            const int x0 = ix * g.sp_x - g.Nx_left + a.f1.mx;
+            const int y1 = iy * g.sp_y + r - g.Ny_left + a.f1.my;
+            float v1[WSX], v2[WSX];
+            load_u8_row<WSX>(a.f1.base + (size_t)y1 * a.f1.pitch + x0, v1);
+            if constexpr (DEF) {
+                load_f32_row<WSX>(a.def + (size_t)(iy * g.sp_y + r) * a.def_pitch + ix * g.sp_x, v2);
+            } else {
+                load_u8_row<WSX>(a.f2.base + (size_t)y1 * a.f2.pitch + x0, v2);
+            }
+#pragma unroll
+            for (int i = 0; i < WSX; ++i) z[i] = make_float2(v1[i], v2[i]);
+        } else {
+#pragma unroll
+            for (int i = 0; i < WSX; ++i) z[i] = make_float2(0.f, 0.f);
+        }
+        fft<WSX, false>(z);
+        float2 *row = sm + (b * WSY + r) * LDX;
+#pragma unroll
+        for (int i = 0; i < WSX; ++i) row[i] = z[i];
+    }
+    __syncthreads();
+
+    // ---------------- P2: forward column FFT ----------------
+    for (int t = tid; t < B * WSX; t += NT) {
+        const int b = t / WSX, c = t - b * WSX;
+        float2 *col = sm + b * WIN + c;
+        float2 z[WSY];
+#pragma unroll
+        for (int r = 0; r < WSY; ++r) z[r] = col[r * LDX];
+        fft<WSY, false>(z);
+#pragma unroll
+        for (int r = 0; r < WSY; ++r) col[r * LDX] = z[r];
+    }
+    __syncthreads();
+
+    // ---------------- P3: cross spectrum of a window pair + inverse column FFT ----------------
+    static_assert((B / 2) * WSX <= NT, "one P3 task per thread");
+    {
+        const bool active = tid < (B / 2) * WSX;
+        const int q = active ? tid / WSX : 0, c = active ? tid - (tid / WSX) * WSX : 0;
+        const int cm = (WSX - c) % WSX;
+        float2 wv[WSY];
+        if (active) {
+            const float2 *za = sm + (2 * q) * WIN, *zb = sm + (2 * q + 1) * WIN;
+#pragma unroll
+            for (int r = 0; r < WSY; ++r) {
+                const int rm = (WSY - r) % WSY;
+                float2 A = za[r * LDX + c], M = za[rm * LDX + cm];
+                // C = Im(A*M)/2 + i*(|M|^2 - |A|^2)/4
+                float2 Ca = make_float2(0.5f * (A.x * M.y + A.y * M.x),
+                                        0.25f * ((M.x * M.x + M.y * M.y) - (A.x * A.x + A.y * A.y)));
+                A = zb[r * LDX + c];
+                M = zb[rm * LDX + cm];
+                float2 Cb = make_float2(0.5f * (A.x * M.y + A.y * M.x),
+                                        0.25f * ((M.x * M.x + M.y * M.y) - (A.x * A.x + A.y * A.y)));
+                wv[r] = make_float2(Ca.x - Cb.y, Ca.y + Cb.x);  // C_a + i*C_b
+            }
+            fft<WSY, true>(wv);
+        }
+        __syncthreads();  // every partner-column read is done
+        if (active) {
+            float2 *col = sm + (2 * q) * WIN + c;
+#pragma unroll
+            for (int r = 0; r < WSY; ++r) col[r * LDX] = wv[r];
+        }
+    }
+    __syncthreads();
+
+    // ---------------- P4: inverse row FFT -> two shifted FP32 planes ----------------
+    for (int t = tid; t < (B / 2) * WSY; t += NT) {
+        const int q = t / WSY, r = t - q * WSY;
+        const float2 *row = sm + (2 * q) * WIN + r * LDX;
+        float2 z[WSX];
+#pragma unroll
+        for (int i = 0; i < WSX; ++i) z[i] = row[i];
+        fft<WSX, true>(z);
+        float *pa = reinterpret_cast<float *>(sm + (2 * q + 1) * WIN);
+        float *pb = pa + WSY * LDF;
+        const int rs = (r + WSY / 2) % WSY;
+#pragma unroll
+        for (int i = 0; i < WSX; ++i) {
+            const int is = (i + WSX / 2) % WSX;
+            pa[rs * LDF + is] = fabsf(z[i].x) * inv_n;
+            pb[rs * LDF + is] = fabsf(z[i].y) * inv_n;
+        }
+    }
+    __syncthreads();
+
+    // ---------------- P5: peaks, warp per window ----------------
+    const int warp = tid >> 5, lane = tid & 31;
+    constexpr int NW = NT / 32;
+    const int rows = WSY - 2 * g.by, cols = WSX - 2 * g.bx;
+    for (int b = warp; b < B; b += NW) {
+        const int w = w_base + b;
+        if (w >= a.w_end) continue;
+        const float *P = reinterpret_cast<const float *>(sm + ((b & ~1) + 1) * WIN) + (b & 1) * (WSY * LDF);
+        float tv[K];
+        int ti[K];
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            tv[k] = -1.f;
+            ti[k] = INT_MAX;
+        }
+        int cnt = 0;
+        const int nreg = rows * cols;
+        for (int t = lane; t < nreg; t += 32) {
+            const int jj = t / cols, ii = t - jj * cols;
+            const int j = g.by + jj, i = g.bx + ii;
+            const float *pr = P + j * LDF + i;
+            const float v = pr[0];
+            if (v > 0.f && v >= pr[-1] && v >= pr[1] && v >= pr[-LDF] && v >= pr[LDF]) {
+                cnt++;
+                topk_insert<K>(tv, ti, v, j * WSX + i);
+            }
+        }
+#pragma unroll
+        for (int off = 16; off >= 1; off >>= 1) {
+            cnt += __shfl_xor_sync(0xffffffffu, cnt, off);
+            float pv[K];
+            int pi[K];
+#pragma unroll
+            for (int k = 0; k < K; ++k) {
+                pv[k] = __shfl_xor_sync(0xffffffffu, tv[k], off);
+                pi[k] = __shfl_xor_sync(0xffffffffu, ti[k], off);
+            }
+#pragma unroll
+            for (int k = 0; k < K; ++k) topk_insert<K>(tv, ti, pv[k], pi[k]);
+        }
+        if (lane < g.Nps) {
+            float v = -1.f;
+            int idx = INT_MAX;
+#pragma unroll
+            for (int k = 0; k < K; ++k)
+                if (k == lane) {
+                    v = tv[k];
+                    idx = ti[k];
+                }
+            float ox = 0.f, oy = 0.f;
+            bool ok = false;
+            if (v > 0.f) {
+                const int j = idx / WSX, i = idx - j * WSX;
+                if (i != 0 && i != WSX - 1 && j != 0 && j != WSY - 1) {
+                    const float *pc = P + j * LDF + i;
+                    const float c0 = pc[-1], c2 = pc[1], d0 = pc[-LDF], d2 = pc[LDF];
+                    const double dv = (double)v * (double)v;
+                    // numerator ln f- - ln f+ in FP32 as the reference; the cancelling
+                    // denominator ln(f- f+ / f0^2) in FP64
+                    const float nx = logf(c0) - logf(c2), ny = logf(d0) - logf(d2);
+                    const double denx = log(((double)c0 * (double)c2) / dv);
+                    const double deny = log(((double)d0 * (double)d2) / dv);
+                    const float sx = (float)((double)nx / denx / 2.0), sy = (float)((double)ny / deny / 2.0);
+                    ox = (float)i + sx - (float)WSX / 2 + a.pred_x[w];
+                    oy = (float)j + sy - (float)WSY / 2 + a.pred_y[w];
+                    ok = true;
+                    if (ox < g.lx1 || ox > g.lx2 || oy < g.ly1 || oy > g.ly2) {
+                        ok = false;
+                        ox = 0.f;
+                        oy = 0.f;
+                    }
+                    if (isnan(ox) || isnan(oy) || isinf(ox) || isinf(oy)) {
+                        ok = false;
+                        ox = 0.f;
+                        oy = 0.f;
+                    }
+                }
+            }
+            const size_t o = (size_t)w * g.Nps + lane;
+            a.cdx[o] = ox;
+            a.cdy[o] = oy;
+            a.cvalid[o] = ok ? 1 : 0;
+            a.pidx[o] = (v > 0.f) ? idx : -1;
+            a.pval[o] = (v > 0.f) ? v : 0.f;
+        }
+        if (lane == 0) a.count[w] = cnt;
+        if (a.cc_dump) {
+            float *dst = a.cc_dump + (size_t)(w - a.w_first) * (WSX * WSY);
+            for (int t = lane; t < WSX * WSY; t += 32) {
+                const int j = t / WSX, i = t - j * WSX;
+                dst[t] = P[j * LDF + i];
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------
+// Launch of one instantiated shape (explicitly instantiated in xcorr_shape_*.cu).
+// ------------------------------------------------------------------------------
+template <int WSX, int WSY, int B, int NT>
+cudaError_t launch_shape(const XcorrArgs &a, bool deformed, int K, cudaStream_t s)
+{
+    const int n = a.w_end - a.w_first;
+    if (n <= 0) return cudaSuccess;
+    const size_t smem = (size_t)B * WSY * (WSX + 1) * sizeof(float2);
+    dim3 grid((n + B - 1) / B);
+    cudaError_t e = cudaSuccess;
+    auto go = [&](auto kern) {
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return;
+        kern<<<grid, NT, smem, s>>>(a);
+        e = cudaGetLastError();
+    };
+    if (K <= 4) {
+        if (deformed) go(xcorr_peak_kernel<WSX, WSY, B, NT, 4, true>);
+        else go(xcorr_peak_kernel<WSX, WSY, B, NT, 4, false>);
+    } else {
+        if (deformed) go(xcorr_peak_kernel<WSX, WSY, B, NT, 8, true>);
+        else go(xcorr_peak_kernel<WSX, WSY, B, NT, 8, false>);
+    }
+    return e;
+}
+
+}  // namespace piv

@@ -1,0 +1,6 @@
+// Fused correlation kernel, 48x24 windows (4 windows and 96 threads per CTA).
+#include "xcorr_kernel.cuh"
+
+namespace piv {
+template cudaError_t launch_shape<48, 24, 4, 96>(const XcorrArgs &, bool, int, cudaStream_t);
+}

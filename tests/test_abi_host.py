@@ -1,0 +1,191 @@
+"""CPU tests of the C-ABI library and the host logic (no GPU compute):
+
+  - the library loads and exports every entry point include/piv_b200.h declares;
+  - the 50-line parameter file parser (X/main.cpp:93-158), including the reference's own
+    "Parameter missing" case (a 41-line file, like x64/Debug/Parameter.dat);
+  - geometry (xcorr2d_multi::init, X/xcorr2d_multi_grid.cu:751-920) against the known
+    grid counts of the reference's sample outputs and against the oracle's restatement;
+  - output file names (X/main.cpp:327-369) against the sample result file names;
+  - the Tecplot writer byte for byte against the oracle's writer and the sample headers;
+  - the synthetic pair generator (determinism, field models).
+"""
+import hashlib
+import re
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import piv_b200 as P
+from oracle import oracle as O
+
+ROOT = Path(__file__).resolve().parents[1]
+
+# The reference's example parameter file (X/Parameter.dat), lines 7..50.
+REF_EXAMPLE = ["0", "1", "40", "0.91", "6600", "4400", "64", "64", "32", "32", "2", "32", "32", "16", "16", "2", "1",
+               "5", "5", "2", "5", "2", "3", "3", "3", "1", "5", "5", "2", "5", "2", "3", "3", "3", "1", "0.4", "0.4",
+               "0.4", "0.4", "4", "-100", "100", "-100", "100"]
+REF_PATHS = ["E:\\data\\1_", ".tif", "E:\\data\\2_", ".tif", "E:\\data\\pair index.txt", "E:\\data\\result\\"]
+
+
+def test_library_exports_every_declared_entry_point():
+    header = (ROOT / "include" / "piv_b200.h").read_text()
+    declared = set(re.findall(r"^(?:int|const char \*)\s*(piv_\w+)\(", header, re.M))
+    assert len(declared) >= 35
+    h = P.lib()
+    for name in declared:
+        assert hasattr(h, name), name
+    assert declared == set(P.EXPORTS), declared ^ set(P.EXPORTS)
+
+
+def _write_params(path, lines, crlf=True):
+    nl = "\r\n" if crlf else "\n"
+    path.write_bytes(nl.join(lines).encode())
+
+
+def test_params_read_reference_example(tmp_path):
+    f = tmp_path / "Parameter.dat"
+    _write_params(f, REF_PATHS + REF_EXAMPLE)
+    p, paths = P.read_params(f)
+    assert paths["prefix_f1"] == "E:\\data\\1_" and paths["suffix_f2"] == ".tif"
+    assert paths["folder_result"] == "E:\\data\\result\\"
+    assert (p.if_mhe, p.mhe_ws, p.Nx, p.Ny) == (1, 40, 6600, 4400)
+    assert abs(p.mhe_thresh - 0.91) < 1e-7
+    assert (p.ws_x1, p.ws_y1, p.spacing_x1, p.Npass1, p.ws_x2, p.spacing_x2, p.Npass2) == (64, 64, 32, 2, 32, 16, 2)
+    assert (p.wx1_median, p.Npass1_median, p.minNneigh_p1, p.insert_threshold_p1) == (5, 2, 5, 3.0)
+    assert (p.wx2_smooth, p.Npass2_smooth, p.Npeak_save) == (3, 1, 4)
+    assert abs(p.max_dispx_win_percent1 - 0.4) < 1e-7
+    assert (p.dispx_lim1, p.dispx_lim2, p.dispy_lim1, p.dispy_lim2) == (-100, 100, -100, 100)
+
+
+def test_params_read_missing_line_and_file(tmp_path):
+    f = tmp_path / "Parameter.dat"
+    _write_params(f, (REF_PATHS + REF_EXAMPLE)[:41], crlf=False)
+    with pytest.raises(P.PivError) as ei:
+        P.read_params(f)
+    assert ei.value.status == P.PIV_ERR_ARG
+    with pytest.raises(P.PivError) as ei:
+        P.read_params(tmp_path / "nope.dat")
+    assert ei.value.status == P.PIV_ERR_IO
+
+
+def test_geometry_known_grid_counts():
+    # the sample outputs of the reference (data/data_organized/result/*.dat headers) at 6600x4400:
+    # spacing 32 -> I=206, J=137; spacing 16 -> I=412, J=275
+    g = P.geometry(P.default_params())
+    assert g["Nx_vec"] == (206, 412) and g["Ny_vec"] == (137, 275)
+    assert g["Nt_vec"] == (206 * 137, 412 * 275)
+    assert g["Npeak"] == (256, 64)
+    # the 1024^2 single-grid case: 64x64 vectors, aug 1040, aug_ex 1072, border 16 - round(8) = 8
+    p = P.default_params(Nx=1024, Ny=1024, ws_x1=32, ws_y1=32, spacing_x1=16, spacing_y1=16,
+                         max_dispx_win_percent1=0.25, max_dispy_win_percent1=0.25)
+    g = P.geometry(p)
+    assert g["Nx_vec"][0] == 64 and g["Nx_aug"][0] == 1040 and g["Nx_aug_ex"][0] == 1072 and g["border_x"][0] == 8
+
+
+def test_geometry_matches_oracle_sweep():
+    rng = np.random.default_rng(0)
+    for _ in range(300):
+        ws = [int(rng.integers(1, 33)) * 4 for _ in range(4)]
+        sp = [int(rng.integers(1, 80)) for _ in range(4)]
+        p = P.default_params(Nx=int(rng.integers(40, 3000)), Ny=int(rng.integers(40, 3000)),
+                             ws_x1=ws[0], ws_y1=ws[1], ws_x2=ws[2], ws_y2=ws[3], spacing_x1=sp[0], spacing_y1=sp[1],
+                             spacing_x2=sp[2], spacing_y2=sp[3], Nsec_cc=int(rng.integers(1, 7)),
+                             max_dispx_win_percent1=float(rng.random()), max_dispy_win_percent1=float(rng.random()),
+                             max_dispx_win_percent2=float(rng.random()), max_dispy_win_percent2=float(rng.random()))
+        rc, og = O.geometry(O.params_from(p))
+        try:
+            g = P.geometry(p)
+        except P.PivError as err:
+            assert rc != 0, err
+            continue
+        assert rc == 0
+        assert g == og.to_dict()
+
+
+@pytest.mark.parametrize("kw,code", [(dict(ws_x1=2), P.PIV_ERR_GEOMETRY), (dict(ws_y2=2048), P.PIV_ERR_GEOMETRY),
+                                     (dict(ws_x2=30), P.PIV_ERR_GEOMETRY), (dict(Nsec_cc=0), P.PIV_ERR_ARG),
+                                     (dict(Nx=100, Ny=100, Nsec_cc=10**6), P.PIV_ERR_ARG)])
+def test_geometry_rejections(kw, code):
+    with pytest.raises(P.PivError) as ei:
+        P.geometry(P.default_params(**kw))
+    assert ei.value.status == code
+
+
+def test_output_names_match_reference_samples():
+    p = P.default_params()
+    folder = "result/"
+    # file names present in the reference's data/data_organized/result/
+    assert P.output_name(p, folder, 1, 0) == "result/0001_vector_GPU_Grid1_4-peak-candidate_3DCC-64-64-2pass_4peaks_raw.dat"
+    assert (P.output_name(p, folder, 1, 1) ==
+            "result/0001_vector_GPU_Grid1_4-peak-candidate_3DCC-64-64-2pass_median-5-5-3.0-2pass_smooth-3-3-1pass.dat")
+    assert P.output_name(p, folder, 1, 2) == "result/0001_vector_GPU_Grid2_4-peak-candidate_3DCC-32-32-2pass_4peaks_raw.dat"
+    assert (P.output_name(p, folder, 1, 3) ==
+            "result/0001_vector_GPU_Grid2_4-peak-candidate_3DCC-32-32-2pass_median-5-5-3.0-2pass_smooth-3-3-1pass.dat")
+    assert (P.output_name(p, folder, 1, 4) ==
+            "result/0001_vector_GPU_Grid2_4-peak-candidate_3DCC-32-32-2pass_median-5-5-3.0-2pass.dat")
+    assert P.output_name(p, "", 12345, 0).startswith("12345_vector")
+
+
+def test_tecplot_writer_matches_oracle_and_sample_format(tmp_path):
+    rng = np.random.default_rng(1)
+    nx, ny, nps = 13, 7, 4
+    dx = (rng.normal(0, 5, nx * ny * nps)).astype(np.float32)
+    dy = (rng.normal(0, 5, nx * ny * nps)).astype(np.float32)
+    dx[:5] = [0.0, -0.0, -0.004, 0.005, 2.675]
+    for raw in (1, 0):
+        a, b = tmp_path / f"a{raw}.dat", tmp_path / f"b{raw}.dat"
+        rc = P.lib().piv_tecplot_write_arrays(str(a).encode(), nx, ny, 16, 16, raw, nps,
+                                              dx.ctypes.data_as(P._F), dy.ctypes.data_as(P._F))
+        assert rc == 0
+        O.write_tecplot(b, nx, ny, 16, 16, raw, nps, dx, dy)
+        assert a.read_bytes() == b.read_bytes()
+        lines = a.read_text().split("\n")
+        assert lines[0] == 'TITLE = "B00001"'
+        if raw:
+            assert lines[1] == 'VARIABLES = "x", "y", "dx1", "dy1", "dx2", "dy2", "dx3", "dy3", "dx4", "dy4"'
+        else:
+            assert lines[1] == 'VARIABLES = "x", "y", "displacement-x", "displacement-y"'
+        assert lines[2] == f'ZONE T="Frame 0", I={nx}, J={ny}'
+        assert lines[3].startswith("8.00\t8.00\t")
+        assert len(lines[3].split("\t")) == (10 if raw else 4)
+
+
+def test_synth_pair_deterministic_and_seeded():
+    s = P.synth_params(96, 64, ppp=0.05, field=P.PIV_FIELD_UNIFORM, a=3.3, b=-1.7, seed=9)
+    a1, a2 = P.synth_pair(s)
+    b1, b2 = P.synth_pair(s)
+    assert np.array_equal(a1, b1) and np.array_equal(a2, b2)
+    s.seed = 10
+    c1, _ = P.synth_pair(s)
+    assert not np.array_equal(a1, c1)
+    assert 10 <= a1.mean() <= 80 and a1.max() >= 200
+
+
+def test_synth_fixture_checksum():
+    # the golden fixtures regenerate their inputs from seeds; this pins the generator
+    s = P.synth_params(1024, 1024, ppp=0.05, field=P.PIV_FIELD_UNIFORM, a=3.3, b=-1.7, seed=1)
+    f1, f2 = P.synth_pair(s)
+    gold = ROOT / "tests" / "golden" / "golden_c0.npz"
+    if not gold.exists():
+        pytest.skip("golden fixtures not generated yet")
+    z = np.load(gold)
+    assert hashlib.sha256(f1.tobytes()).hexdigest() == str(z["f1_sha"][0])
+    assert hashlib.sha256(f2.tobytes()).hexdigest() == str(z["f2_sha"][0])
+
+
+def test_synth_field_models():
+    s = P.synth_params(1000, 800, field=P.PIV_FIELD_VORTEX, a=10.0, b=100.0, c=0.0)
+    r = np.linspace(1, 400, 2000).astype(np.float32)
+    u, v = P.synth_field(s, 500 + r, np.full_like(r, 400))
+    assert abs(np.abs(v).max() - 10.0) < 1e-3  # peak tangential speed
+    assert abs(r[np.argmax(np.abs(v))] / 100.0 - 1.1209) < 0.01  # at r = 1.1209 rc (Lamb-Oseen)
+    pt = (np.array([500.0], np.float32), np.array([700.0], np.float32))
+    u0, _ = P.synth_field(s, *pt)
+    s.c = 0.002
+    u1, _ = P.synth_field(s, *pt)
+    assert abs((u1[0] - u0[0]) - 0.002 * (700 - 400)) < 1e-5  # linear shear in x
+    s = P.synth_params(1000, 800, field=P.PIV_FIELD_FOURIER, a=200.0, b=2000.0, c=12.0, seed=4)
+    xx, yy = np.meshgrid(np.arange(0, 1000, 10, dtype=np.float32), np.arange(0, 800, 10, dtype=np.float32))
+    u, v = P.synth_field(s, xx.ravel(), yy.ravel())
+    assert np.abs(u).max() <= 12.0 + 1e-4 and np.abs(u).max() > 3.0
