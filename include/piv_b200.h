@@ -187,6 +187,13 @@ int piv_write_tecplot(piv_engine *e, const char *path, int selection);
 int piv_tecplot_write_arrays(const char *path, int Nx_vec, int Ny_vec, int spacing_x, int spacing_y, int raw,
                              int Npeak_save, const float *dx, const float *dy);
 
+/* Baseline TIFF (CImageIO, X/ImageIOPkg.cpp:124-428 and :641): uncompressed, 8-bit grey,
+ * strip-organised, either byte order.  piv_tiff_read8 needs the file to be exactly Nx x Ny
+ * (PIV_ERR_ARG otherwise, PIV_ERR_UNSUPPORTED for other bit depths or compression). */
+int piv_tiff_info(const char *path, int *Nx, int *Ny, int *bits);
+int piv_tiff_read8(const char *path, uint8_t *out, int Nx, int Ny);
+int piv_tiff_write8(const char *path, const uint8_t *img, int Nx, int Ny);
+
 /* Output file name of X/main.cpp:327-369 for pair index `idx`:
  * kind 0 grid-1 raw, 1 grid-1 filtered, 2 grid-2 raw, 3 grid-2 filtered, 4 grid-2 median-only. */
 int piv_output_name(const piv_params *p, const char *folder, int idx, int kind, char *out, size_t cap);
@@ -211,8 +218,8 @@ int piv_get_frames(piv_engine *e, uint8_t *f1, uint8_t *f2);
 int piv_get_deformed(piv_engine *e, int grid, float *out);
 
 /* Re-runs the correlation of the last pass of `grid` for windows [first, first+n) and
- * returns their shifted correlation planes ([n][ws_y][ws_x] floats); the candidates of
- * those windows are rewritten with identical values. */
+ * returns their shifted correlation planes ([n][ws_y][ws_x] floats).  Candidates and
+ * fields are not touched. */
 int piv_debug_cc_planes(piv_engine *e, int grid, int first, int n, float *out);
 
 /* Device time of the kernels of the last piv_run_pair, by stage (ms): [0] prep+MHE,
@@ -225,6 +232,11 @@ int piv_stage_times(piv_engine *e, float *ms5);
 /* The engine's CUDA stream (a cudaStream_t), for callers that order their own work
  * (events, copies) against the engine. */
 int piv_get_stream(const piv_engine *e, void **stream);
+
+/* The fused correlation kernel configuration the autotuner chose for a grid at
+ * piv_create (windows per CTA, threads per CTA) and its measured time per launch on
+ * the tuning input (0 if not tuned; PIV_AUTOTUNE=0 keeps the defaults). */
+int piv_xcorr_config(const piv_engine *e, int grid, int *windows_per_cta, int *threads_per_cta, float *tuned_ms);
 
 /* Kernels that one piv_run_pair launches with the engine's parameters. */
 int piv_kernel_launches_per_pair(const piv_engine *e, int *n);

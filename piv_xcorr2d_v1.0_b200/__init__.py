@@ -120,6 +120,9 @@ EXPORTS = {
     "piv_write_tecplot": (C.c_int, [_P, C.c_char_p, C.c_int]),
     "piv_tecplot_write_arrays": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _F, _F]),
     "piv_output_name": (C.c_int, [C.POINTER(PivParams), C.c_char_p, C.c_int, C.c_int, C.c_char_p, C.c_size_t]),
+    "piv_tiff_info": (C.c_int, [C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "piv_tiff_read8": (C.c_int, [C.c_char_p, _U8, C.c_int, C.c_int]),
+    "piv_tiff_write8": (C.c_int, [C.c_char_p, _U8, C.c_int, C.c_int]),
     "piv_get_peaks": (C.c_int, [_P, C.c_int, _I32, _I32, _F]),
     "piv_set_field": (C.c_int, [_P, C.c_int, _F, _F, _U8]),
     "piv_set_candidates": (C.c_int, [_P, C.c_int, _F, _F, _U8]),
@@ -128,6 +131,7 @@ EXPORTS = {
     "piv_debug_cc_planes": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, _F]),
     "piv_stage_times": (C.c_int, [_P, _F]),
     "piv_get_stream": (C.c_int, [_P, C.POINTER(_P)]),
+    "piv_xcorr_config": (C.c_int, [_P, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), _F]),
     "piv_kernel_launches_per_pair": (C.c_int, [_P, C.POINTER(C.c_int)]),
     "piv_time_stage": (C.c_int, [_P, C.c_int, C.c_int, _F]),
     "piv_probe_fp32_peak": (C.c_int, [_F]),
@@ -408,6 +412,12 @@ class Engine:
         s = C.c_void_p()
         self._ck(lib().piv_get_stream(self.h, C.byref(s)))
         return s.value or 0
+
+    def xcorr_config(self, grid):
+        """(windows per CTA, threads per CTA, tuned ms per launch) of the grid's fused kernel."""
+        b, nt, ms = C.c_int(0), C.c_int(0), C.c_float(0)
+        self._ck(lib().piv_xcorr_config(self.h, grid, C.byref(b), C.byref(nt), C.byref(ms)))
+        return b.value, nt.value, ms.value
 
     def launches_per_pair(self):
         n = C.c_int(0)

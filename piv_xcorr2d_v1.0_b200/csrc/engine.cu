@@ -120,6 +120,9 @@ struct GridState {
     int def_pitch = 0;
     bool last_deformed = false;
     bool has_pass = false;
+    int variant = 0;          // fused-kernel instantiation chosen by the autotuner
+    float tuned_ms[8] = {};   // measured time per variant (0 = not measured)
+    int n_tuned = 0;
 };
 
 struct piv_engine {
@@ -294,7 +297,7 @@ int do_xcorr(piv_engine *e, int k, bool deformed, int first, int end, float *dum
     if (dump) {
         a.w_first = first;
         a.w_end = end;
-        cudaError_t c = launch_xcorr(a, deformed, e->stream, &why);
+        cudaError_t c = launch_xcorr(a, deformed, e->stream, &why, gs.variant);
         if (c != cudaSuccess) return set_err(e, PIV_ERR_CUDA, "correlation kernel: %s", why ? why : cudaGetErrorString(c));
         return PIV_OK;
     }
@@ -303,7 +306,7 @@ int do_xcorr(piv_engine *e, int k, bool deformed, int first, int end, float *dum
     for (int i = 0; i < Nsec; ++i) {
         a.w_first = i * Neach;
         a.w_end = a.w_first + (i == Nsec - 1 ? Nlast : Neach);
-        cudaError_t c = launch_xcorr(a, deformed, e->stream, &why);
+        cudaError_t c = launch_xcorr(a, deformed, e->stream, &why, gs.variant);
         if (c != cudaSuccess) return set_err(e, PIV_ERR_CUDA, "correlation kernel: %s", why ? why : cudaGetErrorString(c));
     }
     return PIV_OK;
@@ -435,6 +438,69 @@ int do_pair(piv_engine *e, bool with_events)
     }
     mark(3);
     return PIV_OK;
+}
+
+// The autotuner: every instantiated variant (windows per CTA, threads per CTA) of each
+// grid's window shape is timed on this engine's own geometry, with the frames (and the
+// deformed frame, the mode most passes run in) holding a particle-like pattern; the
+// fastest variant is kept.  PIV_AUTOTUNE=0 keeps the defaults.
+int tune_xcorr(piv_engine *e)
+{
+    const char *env = getenv("PIV_AUTOTUNE");
+    if (env && atoi(env) == 0) return PIV_OK;
+    const piv_params &p = e->p;
+    cudaStream_t s = e->stream;
+    CK(launch_pattern(e->d_f1, nullptr, e->pitch, e->pitch, e->rows, 1u, s));
+    CK(launch_pattern(e->d_f2, nullptr, e->pitch, e->pitch, e->rows, 2u, s));
+    cudaEvent_t a, b;
+    CK(cudaEventCreate(&a));
+    CK(cudaEventCreate(&b));
+    int rc = PIV_OK;
+    for (int k = 0; k < 2 && !rc; ++k) {
+        GridState &gs = e->grid[k];
+        if ((k == 0 ? p.Npass1 : p.Npass2) < 1) continue;
+        const int nv = xcorr_variants(gs.gg.ws_x, gs.gg.ws_y);
+        if (nv <= 1) continue;
+        const bool deformed = gs.def != nullptr;
+        if (deformed) CK(launch_pattern(nullptr, gs.def, gs.def_pitch, gs.gg.Nx_aug, gs.gg.Ny_aug, 3u + k, s));
+        float best = 1e30f;
+        int best_v = 0;
+        for (int v = 0; v < nv && v < 8 && !rc; ++v) {
+            gs.variant = v;
+            if ((rc = do_xcorr(e, k, deformed, 0, 0, nullptr))) break;  // warm-up
+            cudaEventRecord(a, s);
+            for (int r = 0; r < 2 && !rc; ++r) rc = do_xcorr(e, k, deformed, 0, 0, nullptr);
+            cudaEventRecord(b, s);
+            if (cudaEventSynchronize(b) != cudaSuccess) {
+                rc = set_err(e, PIV_ERR_CUDA, "autotune timing failed");
+                break;
+            }
+            float ms = 0;
+            cudaEventElapsedTime(&ms, a, b);
+            gs.tuned_ms[v] = ms / 2;
+            if (ms < best) {
+                best = ms;
+                best_v = v;
+            }
+        }
+        gs.variant = best_v;
+        gs.n_tuned = nv < 8 ? nv : 8;
+        // leave no trace of the tuning input
+        if (deformed) CK(cudaMemsetAsync(gs.def, 0, (size_t)gs.def_pitch * gs.gg.Ny_aug * sizeof(float), s));
+        const size_t Nt = (size_t)gs.gg.Nt_vec, Nc = Nt * p.Npeak_save;
+        CK(cudaMemsetAsync(gs.cdx, 0, Nc * sizeof(float), s));
+        CK(cudaMemsetAsync(gs.cdy, 0, Nc * sizeof(float), s));
+        CK(cudaMemsetAsync(gs.cv, 0, Nc, s));
+        CK(cudaMemsetAsync(gs.count, 0, Nt * sizeof(int), s));
+        CK(cudaMemsetAsync(gs.pidx, 0xff, Nc * sizeof(int), s));
+        CK(cudaMemsetAsync(gs.pval, 0, Nc * sizeof(float), s));
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    CK(cudaMemsetAsync(e->d_f1, 0, (size_t)e->pitch * e->rows, s));
+    CK(cudaMemsetAsync(e->d_f2, 0, (size_t)e->pitch * e->rows, s));
+    CK(cudaStreamSynchronize(s));
+    return rc;
 }
 
 int validate_params(piv_engine *e, const piv_params &p)
@@ -598,6 +664,7 @@ int piv_create(const piv_params *p, piv_engine **out)
             cudaMemset(gs.def, 0, nd * sizeof(float));
         }
     }
+    if ((rc = tune_xcorr(e))) return bail(rc);
     if (getenv("PIV_TIMING") && atoi(getenv("PIV_TIMING")) == 1) {
         e->timing = true;
         for (auto &ev : e->ev) cudaEventCreate(&ev);
@@ -914,6 +981,16 @@ int piv_debug_cc_planes(piv_engine *e, int grid, int first, int n, float *out)
 }
 
 // ---- measurement -----------------------------------------------------------------
+
+int piv_xcorr_config(const piv_engine *e, int grid, int *windows_per_cta, int *threads_per_cta, float *tuned_ms)
+{
+    if (!e || grid < 0 || grid > 1) return PIV_ERR_ARG;
+    const GridState &gs = e->grid[grid];
+    if (!xcorr_variant_shape(gs.gg.ws_x, gs.gg.ws_y, gs.variant, windows_per_cta, threads_per_cta))
+        return PIV_ERR_UNSUPPORTED;
+    if (tuned_ms) *tuned_ms = gs.n_tuned ? gs.tuned_ms[gs.variant] : 0.f;
+    return PIV_OK;
+}
 
 int piv_get_stream(const piv_engine *e, void **stream)
 {

@@ -99,6 +99,36 @@ cudaError_t launch_deform(const DeformArgs &a, cudaStream_t s)
 }
 
 // ------------------------------------------------------------------------------
+// Autotuning input: a particle-like pattern (sparse bright pixels on a dark
+// background) so that the timed correlation does its full candidate work.
+// ------------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t hash2(uint32_t x, uint32_t y)
+{
+    uint32_t h = x * 0x9E3779B1u ^ (y + 0x7F4A7C15u) * 0x85EBCA77u;
+    h ^= h >> 15;
+    h *= 0x2C1B3C6Du;
+    h ^= h >> 12;
+    return h;
+}
+
+__global__ void pattern_kernel(uint8_t *u8, float *f32, int pitch, int cols, int rows, uint32_t seed)
+{
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+    if (x >= cols || y >= rows) return;
+    const uint32_t h = hash2((uint32_t)x + seed, (uint32_t)y);
+    const float v = (h % 23u == 0u) ? (float)(120u + (h >> 24) % 136u) : (float)(8u + (h >> 28));
+    if (u8) u8[(size_t)y * pitch + x] = (uint8_t)v;
+    if (f32) f32[(size_t)y * pitch + x] = v;
+}
+
+cudaError_t launch_pattern(uint8_t *u8, float *f32, int pitch, int cols, int rows, uint32_t seed, cudaStream_t s)
+{
+    dim3 grid((cols + 255) / 256, rows);
+    pattern_kernel<<<grid, 256, 0, s>>>(u8, f32, pitch, cols, rows, seed);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------------------
 // Upsampling_vecfield_kernel_2d (X/xcorr2d_multi_grid.cu:675-704) with the launch
 // arguments of Upsampling_vector_field (:1580-1581).
 // ------------------------------------------------------------------------------

@@ -1,4 +1,5 @@
 // io.cpp -- parameter file, output naming and the Tecplot writer (host only).
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -143,40 +144,254 @@ int piv_output_name(const piv_params *p, const char *folder, int idx, int kind, 
     return (n < 0 || (size_t)n >= cap) ? PIV_ERR_ARG : PIV_OK;
 }
 
+namespace {
+
+// "%.2f" of a float without printf: f*100 is exact in double (24 + 7 significant
+// bits), rint() rounds it half-to-even in the default rounding mode exactly as printf
+// rounds the exact decimal value, and the sign of negative values that round to zero is
+// kept ("-0.00").  Non-finite values fall back to snprintf.
+char *fmt2(char *p, float f)
+{
+    if (!std::isfinite(f)) return p + std::sprintf(p, "%.2f", (double)f);
+    double t = std::rint((double)f * 100.0);
+    if (std::signbit(f)) *p++ = '-';
+    unsigned long long v = (unsigned long long)std::fabs(t);
+    char tmp[32];
+    int n = 0;
+    unsigned long long ip = v / 100;
+    unsigned fr = (unsigned)(v % 100);
+    do {
+        tmp[n++] = (char)('0' + ip % 10);
+        ip /= 10;
+    } while (ip);
+    while (n) *p++ = tmp[--n];
+    *p++ = '.';
+    *p++ = (char)('0' + fr / 10);
+    *p++ = (char)('0' + fr % 10);
+    return p;
+}
+
+}  // namespace
+
 // Tecplot ASCII body of write_vec_data_general (X/xcorr2d_multi_grid.cu:1875-1886,
 // :1902-1911): setprecision(2) fixed == "%.2f", tab separated, '\n' line ends.
 int piv_tecplot_write_arrays(const char *path, int Nx_vec, int Ny_vec, int sp_x, int sp_y, int raw, int Npeak_save,
                              const float *dx, const float *dy)
 {
-    if (!path || !dx || !dy || Nx_vec < 1 || Ny_vec < 1) return PIV_ERR_ARG;
+    if (!path || !dx || !dy || Nx_vec < 1 || Ny_vec < 1 || Npeak_save < 1) return PIV_ERR_ARG;
     FILE *f = fopen(path, "wb");
     if (!f) return PIV_ERR_IO;  // "Error occurs while the vector file is being written."
-    std::vector<char> buf(1 << 20);
-    setvbuf(f, buf.data(), _IOFBF, buf.size());
-    fputs("TITLE = \"B00001\"\n", f);
-    if (raw)
-        fputs("VARIABLES = \"x\", \"y\", \"dx1\", \"dy1\", \"dx2\", \"dy2\", \"dx3\", \"dy3\", \"dx4\", \"dy4\"\n", f);
-    else
-        fputs("VARIABLES = \"x\", \"y\", \"displacement-x\", \"displacement-y\"\n", f);
-    fprintf(f, "ZONE T=\"Frame 0\", I=%d, J=%d\n", Nx_vec, Ny_vec);
+    std::string out;
     const long Nt = (long)Nx_vec * Ny_vec, n = Nt * (raw ? Npeak_save : 1);
+    out.reserve((size_t)Nt * (raw ? 80 : 36) + 256);
+    out += "TITLE = \"B00001\"\n";
+    if (raw)
+        out += "VARIABLES = \"x\", \"y\", \"dx1\", \"dy1\", \"dx2\", \"dy2\", \"dx3\", \"dy3\", \"dx4\", \"dy4\"\n";
+    else
+        out += "VARIABLES = \"x\", \"y\", \"displacement-x\", \"displacement-y\"\n";
+    char line[512];
+    std::snprintf(line, sizeof(line), "ZONE T=\"Frame 0\", I=%d, J=%d\n", Nx_vec, Ny_vec);
+    out += line;
     for (long i = 0; i < Nt; ++i) {
         const long j = i / Nx_vec, k = i - j * Nx_vec;
-        fprintf(f, "%.2f\t%.2f", (double)(float)(sp_x / 2 + k * sp_x), (double)(float)(sp_y / 2 + j * sp_y));
+        char *p = line;
+        p = fmt2(p, (float)(sp_x / 2 + k * sp_x));
+        *p++ = '\t';
+        p = fmt2(p, (float)(sp_y / 2 + j * sp_y));
         if (raw) {
             // the reference always prints four candidate columns at i*Npeak_save + c
             for (int c = 0; c < 4; ++c) {
                 const long q = i * Npeak_save + c;
-                fprintf(f, "\t%.2f\t%.2f", q < n ? (double)dx[q] : 0.0, q < n ? (double)dy[q] : 0.0);
+                *p++ = '\t';
+                p = fmt2(p, q < n ? dx[q] : 0.f);
+                *p++ = '\t';
+                p = fmt2(p, q < n ? dy[q] : 0.f);
             }
         } else {
-            fprintf(f, "\t%.2f\t%.2f", (double)dx[i], (double)dy[i]);
+            *p++ = '\t';
+            p = fmt2(p, dx[i]);
+            *p++ = '\t';
+            p = fmt2(p, dy[i]);
         }
-        fputc('\n', f);
+        *p++ = '\n';
+        out.append(line, (size_t)(p - line));
     }
-    int bad = ferror(f);
+    const bool ok = std::fwrite(out.data(), 1, out.size(), f) == out.size();
+    const bool closed = std::fclose(f) == 0;
+    return (ok && closed) ? PIV_OK : PIV_ERR_IO;
+}
+
+// ---- minimal baseline TIFF (uncompressed, 8-bit grey, strips; both byte orders) ----
+
+namespace {
+
+struct TiffReader {
+    std::vector<uint8_t> d;
+    bool le = true;
+    uint32_t u16(size_t o) const
+    {
+        return le ? (uint32_t)d[o] | ((uint32_t)d[o + 1] << 8) : ((uint32_t)d[o] << 8) | d[o + 1];
+    }
+    uint32_t u32(size_t o) const
+    {
+        return le ? (uint32_t)d[o] | ((uint32_t)d[o + 1] << 8) | ((uint32_t)d[o + 2] << 16) | ((uint32_t)d[o + 3] << 24)
+                  : ((uint32_t)d[o] << 24) | ((uint32_t)d[o + 1] << 16) | ((uint32_t)d[o + 2] << 8) | d[o + 3];
+    }
+    bool ok(size_t o, size_t n) const { return o + n <= d.size(); }
+};
+
+struct TiffInfo {
+    uint32_t width = 0, height = 0, bits = 8, spp = 1, compression = 1, rows_per_strip = 0;
+    std::vector<uint32_t> offsets, counts;
+};
+
+int tiff_parse(const char *path, TiffReader &r, TiffInfo &t)
+{
+    FILE *f = fopen(path, "rb");
+    if (!f) return PIV_ERR_IO;
+    fseek(f, 0, SEEK_END);
+    long sz = ftell(f);
+    fseek(f, 0, SEEK_SET);
+    if (sz < 8) {
+        fclose(f);
+        return PIV_ERR_IO;
+    }
+    r.d.resize((size_t)sz);
+    size_t got = fread(r.d.data(), 1, (size_t)sz, f);
     fclose(f);
-    return bad ? PIV_ERR_IO : PIV_OK;
+    if (got != (size_t)sz) return PIV_ERR_IO;
+    if (r.d[0] == 'I' && r.d[1] == 'I') r.le = true;
+    else if (r.d[0] == 'M' && r.d[1] == 'M') r.le = false;
+    else return PIV_ERR_IO;
+    if (r.u16(2) != 42) return PIV_ERR_IO;
+    size_t ifd = r.u32(4);
+    if (!r.ok(ifd, 2)) return PIV_ERR_IO;
+    const uint32_t ne = r.u16(ifd);
+    for (uint32_t i = 0; i < ne; ++i) {
+        const size_t e = ifd + 2 + 12 * i;
+        if (!r.ok(e, 12)) return PIV_ERR_IO;
+        const uint32_t tag = r.u16(e), type = r.u16(e + 2), cnt = r.u32(e + 4);
+        const uint32_t esz = type == 3 ? 2 : (type == 4 ? 4 : (type == 1 ? 1 : 0));
+        if (esz == 0) continue;
+        const size_t base = (size_t)cnt * esz <= 4 ? e + 8 : r.u32(e + 8);
+        if (!r.ok(base, (size_t)cnt * esz)) return PIV_ERR_IO;
+        auto val = [&](uint32_t k) -> uint32_t {
+            return esz == 2 ? r.u16(base + 2 * k) : (esz == 4 ? r.u32(base + 4 * k) : r.d[base + k]);
+        };
+        switch (tag) {
+        case 256: t.width = val(0); break;
+        case 257: t.height = val(0); break;
+        case 258: t.bits = val(0); break;
+        case 259: t.compression = val(0); break;
+        case 277: t.spp = val(0); break;
+        case 278: t.rows_per_strip = val(0); break;
+        case 273:
+            t.offsets.resize(cnt);
+            for (uint32_t k = 0; k < cnt; ++k) t.offsets[k] = val(k);
+            break;
+        case 279:
+            t.counts.resize(cnt);
+            for (uint32_t k = 0; k < cnt; ++k) t.counts[k] = val(k);
+            break;
+        default: break;
+        }
+    }
+    return PIV_OK;
+}
+
+void put16(std::vector<uint8_t> &b, uint32_t v)
+{
+    b.push_back((uint8_t)v);
+    b.push_back((uint8_t)(v >> 8));
+}
+
+void put32(std::vector<uint8_t> &b, uint32_t v)
+{
+    put16(b, v & 0xffff);
+    put16(b, v >> 16);
+}
+
+}  // namespace
+
+int piv_tiff_info(const char *path, int *Nx, int *Ny, int *bits)
+{
+    if (!path) return PIV_ERR_ARG;
+    TiffReader r;
+    TiffInfo t;
+    int rc = tiff_parse(path, r, t);
+    if (rc) return rc;
+    if (Nx) *Nx = (int)t.width;
+    if (Ny) *Ny = (int)t.height;
+    if (bits) *bits = (int)t.bits;
+    return PIV_OK;
+}
+
+// CImageIO::getImHeadTiff + ImReadTiff8 (X/ImageIOPkg.cpp:124, :280): an 8-bit grey,
+// uncompressed, strip-organised TIFF of exactly Nx x Ny pixels into out (row-major).
+int piv_tiff_read8(const char *path, uint8_t *out, int Nx, int Ny)
+{
+    if (!path || !out || Nx < 1 || Ny < 1) return PIV_ERR_ARG;
+    TiffReader r;
+    TiffInfo t;
+    int rc = tiff_parse(path, r, t);
+    if (rc) return rc;
+    if (t.width != (uint32_t)Nx || t.height != (uint32_t)Ny) return PIV_ERR_ARG;
+    if (t.bits != 8 || t.spp != 1 || t.compression != 1) return PIV_ERR_UNSUPPORTED;
+    if (t.offsets.empty()) return PIV_ERR_IO;
+    if (t.counts.size() != t.offsets.size()) {
+        // StripByteCounts missing: strips of rows_per_strip rows
+        const uint32_t rps = t.rows_per_strip ? t.rows_per_strip : (uint32_t)Ny;
+        t.counts.assign(t.offsets.size(), rps * (uint32_t)Nx);
+    }
+    const size_t need = (size_t)Nx * Ny;
+    size_t pos = 0;
+    for (size_t s = 0; s < t.offsets.size() && pos < need; ++s) {
+        size_t n = t.counts[s];
+        if (n > need - pos) n = need - pos;
+        if (!r.ok(t.offsets[s], n)) return PIV_ERR_IO;
+        std::memcpy(out + pos, r.d.data() + t.offsets[s], n);
+        pos += n;
+    }
+    return pos == need ? PIV_OK : PIV_ERR_IO;
+}
+
+// ImWriteTiff8 (X/ImageIOPkg.cpp:641): little-endian, one strip, 8-bit grey.
+int piv_tiff_write8(const char *path, const uint8_t *img, int Nx, int Ny)
+{
+    if (!path || !img || Nx < 1 || Ny < 1) return PIV_ERR_ARG;
+    std::vector<uint8_t> b;
+    const uint32_t n = (uint32_t)Nx * (uint32_t)Ny, ntag = 9, ifd = 8, data = ifd + 2 + ntag * 12 + 4;
+    b.push_back('I');
+    b.push_back('I');
+    put16(b, 42);
+    put32(b, ifd);
+    put16(b, ntag);
+    auto tag = [&](uint32_t id, uint32_t type, uint32_t v) {
+        put16(b, id);
+        put16(b, type);
+        put32(b, 1);
+        if (type == 3) {
+            put16(b, v);
+            put16(b, 0);
+        } else {
+            put32(b, v);
+        }
+    };
+    tag(256, 4, (uint32_t)Nx);
+    tag(257, 4, (uint32_t)Ny);
+    tag(258, 3, 8);
+    tag(259, 3, 1);
+    tag(262, 3, 1);
+    tag(273, 4, data);
+    tag(277, 3, 1);
+    tag(278, 4, (uint32_t)Ny);
+    tag(279, 4, n);
+    put32(b, 0);
+    b.insert(b.end(), img, img + n);
+    FILE *f = fopen(path, "wb");
+    if (!f) return PIV_ERR_IO;
+    const bool ok = fwrite(b.data(), 1, b.size(), f) == b.size();
+    return (fclose(f) == 0 && ok) ? PIV_OK : PIV_ERR_IO;
 }
 
 int piv_write_tecplot(piv_engine *e, const char *path, int selection)

@@ -128,9 +128,12 @@ struct XcorrArgs {
 };
 
 // Launches the fused correlation + peak kernel for the window range of a.
-// deformed: frame 2 comes from a.def (float) instead of a.f2 (uint8).
-cudaError_t launch_xcorr(const XcorrArgs &a, bool deformed, cudaStream_t s, const char **why);
+// deformed: frame 2 comes from a.def (float) instead of a.f2 (uint8).  variant selects
+// one of the shape's instantiations (windows per CTA, threads per CTA); 0 = default.
+cudaError_t launch_xcorr(const XcorrArgs &a, bool deformed, cudaStream_t s, const char **why, int variant);
 bool xcorr_supported(int ws_x, int ws_y);
+int xcorr_variants(int ws_x, int ws_y);
+bool xcorr_variant_shape(int ws_x, int ws_y, int variant, int *windows_per_cta, int *threads_per_cta);
 
 // Field kernels (field_kernels.cu).
 struct DeformArgs {
@@ -143,6 +146,10 @@ struct DeformArgs {
     int sp_x, sp_y, hfws_x, hfws_y, Nx_left, Ny_left;
 };
 cudaError_t launch_deform(const DeformArgs &a, cudaStream_t s);
+
+// Fills a uint8 and/or float buffer ([rows][pitch], first `cols` columns) with a
+// particle-like pattern (autotuning input).
+cudaError_t launch_pattern(uint8_t *u8, float *f32, int pitch, int cols, int rows, uint32_t seed, cudaStream_t s);
 
 struct UpsampleArgs {
     const float *fx1, *fy1;

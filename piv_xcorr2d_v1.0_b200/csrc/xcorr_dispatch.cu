@@ -1,6 +1,7 @@
-// xcorr_dispatch.cu -- window shape -> instantiated fused correlation kernel.
-// Each shape (WSX, WSY) is compiled in its own translation unit (xcorr_shape_*.cu)
-// with B windows per CTA and NT threads per CTA.
+// xcorr_dispatch.cu -- window shape and variant -> instantiated fused correlation kernel.
+// Every shape (WSX, WSY) is compiled in its own translation unit (xcorr_shape_*.cu) in
+// several variants (B windows per CTA, NT threads per CTA); the first listed variant of a
+// shape is its default, the engine's autotuner may pick another one per grid.
 #include "piv_common.cuh"
 
 namespace piv {
@@ -8,47 +9,114 @@ namespace piv {
 template <int WSX, int WSY, int B, int NT>
 cudaError_t launch_shape(const XcorrArgs &a, bool deformed, int K, cudaStream_t s);
 
-#define PIV_XCORR_SHAPES(X) \
+#define PIV_XCORR_VARIANTS(X) \
     X(8, 8, 32, 128) \
+    X(8, 8, 16, 128) \
+    X(8, 8, 32, 256) \
     X(12, 12, 16, 96) \
+    X(12, 12, 8, 96) \
+    X(12, 12, 16, 192) \
     X(16, 16, 16, 128) \
+    X(16, 16, 8, 128) \
+    X(16, 16, 16, 256) \
+    X(16, 16, 4, 64) \
     X(24, 24, 8, 96) \
+    X(24, 24, 4, 96) \
+    X(24, 24, 8, 192) \
+    X(24, 24, 2, 64) \
     X(32, 32, 8, 128) \
+    X(32, 32, 4, 128) \
+    X(32, 32, 2, 64) \
+    X(32, 32, 8, 256) \
+    X(32, 32, 4, 64) \
     X(48, 48, 4, 96) \
+    X(48, 48, 2, 96) \
+    X(48, 48, 2, 64) \
+    X(48, 48, 4, 192) \
+    X(64, 64, 2, 128) \
     X(64, 64, 4, 128) \
+    X(64, 64, 2, 64) \
+    X(64, 64, 4, 256) \
     X(48, 24, 4, 96) \
+    X(48, 24, 2, 64) \
+    X(48, 24, 2, 96) \
+    X(48, 24, 8, 192) \
     X(24, 48, 4, 96) \
+    X(24, 48, 2, 64) \
+    X(24, 48, 4, 64) \
+    X(24, 48, 8, 96) \
     X(32, 16, 8, 128) \
+    X(32, 16, 4, 64) \
+    X(32, 16, 8, 256) \
     X(16, 32, 8, 128) \
+    X(16, 32, 4, 64) \
+    X(16, 32, 8, 256) \
     X(64, 32, 4, 128) \
-    X(32, 64, 4, 128)
+    X(64, 32, 2, 64) \
+    X(64, 32, 2, 128) \
+    X(32, 64, 4, 128) \
+    X(32, 64, 2, 64) \
+    X(32, 64, 2, 128)
 
 #define PIV_X(WX, WY, B, NT) extern template cudaError_t launch_shape<WX, WY, B, NT>(const XcorrArgs &, bool, int, cudaStream_t);
-PIV_XCORR_SHAPES(PIV_X)
+PIV_XCORR_VARIANTS(PIV_X)
 #undef PIV_X
 
-bool xcorr_supported(int wsx, int wsy)
-{
-#define PIV_X(WX, WY, B, NT) \
-    if (wsx == WX && wsy == WY) return true;
-    PIV_XCORR_SHAPES(PIV_X)
+namespace {
+struct Variant {
+    int wsx, wsy, B, NT;
+    cudaError_t (*fn)(const XcorrArgs &, bool, int, cudaStream_t);
+};
+const Variant kVariants[] = {
+#define PIV_X(WX, WY, B, NT) {WX, WY, B, NT, &launch_shape<WX, WY, B, NT>},
+    PIV_XCORR_VARIANTS(PIV_X)
 #undef PIV_X
-    return false;
+};
+constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
+
+const Variant *find(int wsx, int wsy, int v)
+{
+    int seen = 0;
+    for (int i = 0; i < kNumVariants; ++i)
+        if (kVariants[i].wsx == wsx && kVariants[i].wsy == wsy) {
+            if (seen == v) return &kVariants[i];
+            ++seen;
+        }
+    return nullptr;
+}
+}  // namespace
+
+int xcorr_variants(int wsx, int wsy)
+{
+    int n = 0;
+    for (int i = 0; i < kNumVariants; ++i) n += (kVariants[i].wsx == wsx && kVariants[i].wsy == wsy);
+    return n;
 }
 
-cudaError_t launch_xcorr(const XcorrArgs &a, bool deformed, cudaStream_t s, const char **why)
+bool xcorr_supported(int wsx, int wsy) { return xcorr_variants(wsx, wsy) > 0; }
+
+bool xcorr_variant_shape(int wsx, int wsy, int variant, int *B, int *NT)
+{
+    const Variant *v = find(wsx, wsy, variant);
+    if (!v) return false;
+    if (B) *B = v->B;
+    if (NT) *NT = v->NT;
+    return true;
+}
+
+cudaError_t launch_xcorr(const XcorrArgs &a, bool deformed, cudaStream_t s, const char **why, int variant)
 {
     if (a.g.Nps > 8) {
         if (why) *why = "Npeak_save > 8 is not built into this engine";
         return cudaErrorInvalidValue;
     }
-    const int K = a.g.Nps <= 4 ? 4 : 8;
-#define PIV_X(WX, WY, B, NT) \
-    if (a.g.ws_x == WX && a.g.ws_y == WY) return launch_shape<WX, WY, B, NT>(a, deformed, K, s);
-    PIV_XCORR_SHAPES(PIV_X)
-#undef PIV_X
-    if (why) *why = "window shape not built into this engine";
-    return cudaErrorInvalidValue;
+    const Variant *v = find(a.g.ws_x, a.g.ws_y, variant);
+    if (!v) v = find(a.g.ws_x, a.g.ws_y, 0);
+    if (!v) {
+        if (why) *why = "window shape not built into this engine";
+        return cudaErrorInvalidValue;
+    }
+    return v->fn(a, deformed, a.g.Nps <= 4 ? 4 : 8, s);
 }
 
 }  // namespace piv

@@ -114,6 +114,7 @@ template <int WSX, int WSY, int B, int NT, int K, bool DEF>
 __global__ void __launch_bounds__(NT) xcorr_peak_kernel(const XcorrArgs a)
 {
     static_assert(B % 2 == 0, "windows are processed in pairs");
+    static_assert(NT % 32 == 0, "the peak stage works in whole warps");
     constexpr int LDX = WSX + 1;   // complex row stride (odd -> conflict-free rows and columns)
     constexpr int WIN = WSY * LDX; // complex elements per window buffer
     constexpr int LDF = WSX + 1;   // float row stride of the correlation planes
@@ -227,6 +228,15 @@ __global__ void __launch_bounds__(NT) xcorr_peak_kernel(const XcorrArgs a)
         const int w = w_base + b;
         if (w >= a.w_end) continue;
         const float *P = reinterpret_cast<const float *>(sm + ((b & ~1) + 1) * WIN) + (b & 1) * (WSY * LDF);
+        if (a.cc_dump) {
+            // diagnostic mode: planes only, the pass outputs stay untouched
+            float *dst = a.cc_dump + (size_t)(w - a.w_first) * (WSX * WSY);
+            for (int t = lane; t < WSX * WSY; t += 32) {
+                const int j = t / WSX, i = t - j * WSX;
+                dst[t] = P[j * LDF + i];
+            }
+            continue;
+        }
         float tv[K];
         int ti[K];
 #pragma unroll
@@ -305,13 +315,6 @@ __global__ void __launch_bounds__(NT) xcorr_peak_kernel(const XcorrArgs a)
             a.pval[o] = (v > 0.f) ? v : 0.f;
         }
         if (lane == 0) a.count[w] = cnt;
-        if (a.cc_dump) {
-            float *dst = a.cc_dump + (size_t)(w - a.w_first) * (WSX * WSY);
-            for (int t = lane; t < WSX * WSY; t += 32) {
-                const int j = t / WSX, i = t - j * WSX;
-                dst[t] = P[j * LDF + i];
-            }
-        }
     }
 }
 

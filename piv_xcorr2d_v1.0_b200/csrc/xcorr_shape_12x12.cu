@@ -1,6 +1,9 @@
-// Fused correlation kernel, 12x12 windows (16 windows and 96 threads per CTA).
+// Fused correlation kernel, 12x12 windows: the (windows per CTA, threads per CTA)
+// variants the autotuner chooses from.
 #include "xcorr_kernel.cuh"
 
 namespace piv {
 template cudaError_t launch_shape<12, 12, 16, 96>(const XcorrArgs &, bool, int, cudaStream_t);
+template cudaError_t launch_shape<12, 12, 8, 96>(const XcorrArgs &, bool, int, cudaStream_t);
+template cudaError_t launch_shape<12, 12, 16, 192>(const XcorrArgs &, bool, int, cudaStream_t);
 }

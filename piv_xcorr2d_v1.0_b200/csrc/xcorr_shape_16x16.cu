@@ -1,6 +1,10 @@
-// Fused correlation kernel, 16x16 windows (16 windows and 128 threads per CTA).
+// Fused correlation kernel, 16x16 windows: the (windows per CTA, threads per CTA)
+// variants the autotuner chooses from.
 #include "xcorr_kernel.cuh"
 
 namespace piv {
 template cudaError_t launch_shape<16, 16, 16, 128>(const XcorrArgs &, bool, int, cudaStream_t);
+template cudaError_t launch_shape<16, 16, 8, 128>(const XcorrArgs &, bool, int, cudaStream_t);
+template cudaError_t launch_shape<16, 16, 16, 256>(const XcorrArgs &, bool, int, cudaStream_t);
+template cudaError_t launch_shape<16, 16, 4, 64>(const XcorrArgs &, bool, int, cudaStream_t);
 }

@@ -1,6 +1,9 @@
-// Fused correlation kernel, 16x32 windows (8 windows and 128 threads per CTA).
+// Fused correlation kernel, 16x32 windows: the (windows per CTA, threads per CTA)
+// variants the autotuner chooses from.
 #include "xcorr_kernel.cuh"
 
 namespace piv {
 template cudaError_t launch_shape<16, 32, 8, 128>(const XcorrArgs &, bool, int, cudaStream_t);
+template cudaError_t launch_shape<16, 32, 4, 64>(const XcorrArgs &, bool, int, cudaStream_t);
+template cudaError_t launch_shape<16, 32, 8, 256>(const XcorrArgs &, bool, int, cudaStream_t);
 }

@@ -1,6 +1,10 @@
-// Fused correlation kernel, 24x48 windows (4 windows and 96 threads per CTA).
+// Fused correlation kernel, 24x48 windows: the (windows per CTA, threads per CTA)
+// variants the autotuner chooses from.
 #include "xcorr_kernel.cuh"
 
 namespace piv {
 template cudaError_t launch_shape<24, 48, 4, 96>(const XcorrArgs &, bool, int, cudaStream_t);
+template cudaError_t launch_shape<24, 48, 2, 64>(const XcorrArgs &, bool, int, cudaStream_t);
+template cudaError_t launch_shape<24, 48, 4, 64>(const XcorrArgs &, bool, int, cudaStream_t);
+template cudaError_t launch_shape<24, 48, 8, 96>(const XcorrArgs &, bool, int, cudaStream_t);
 }

@@ -1,6 +1,9 @@
-// Fused correlation kernel, 8x8 windows (32 windows and 128 threads per CTA).
+// Fused correlation kernel, 8x8 windows: the (windows per CTA, threads per CTA)
+// variants the autotuner chooses from.
 #include "xcorr_kernel.cuh"
 
 namespace piv {
 template cudaError_t launch_shape<8, 8, 32, 128>(const XcorrArgs &, bool, int, cudaStream_t);
+template cudaError_t launch_shape<8, 8, 16, 128>(const XcorrArgs &, bool, int, cudaStream_t);
+template cudaError_t launch_shape<8, 8, 32, 256>(const XcorrArgs &, bool, int, cudaStream_t);
 }

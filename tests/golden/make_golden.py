@@ -81,6 +81,15 @@ def make_case(name, sk, pk, outdir):
             out[f"peaks{k}_count"], out[f"peaks{k}_index"], out[f"peaks{k}_value"] = cnt, idx, val
             fx, fy, fv = r.filtered(k, nt)
             out[f"filt{k}_dx"], out[f"filt{k}_dy"], out[f"filt{k}_valid"] = fx, fy, fv
+        if name in ("c0", "multigrid"):
+            # write_vec_data_general's own files, to pin the Tecplot format byte for byte
+            import tempfile
+
+            with tempfile.TemporaryDirectory() as td:
+                for sel in range(4 if p.Npass2 > 0 else 2):
+                    fn = Path(td) / f"sel{sel}.dat"
+                    r.write_tecplot(fn, sel)
+                    out[f"tecplot_sel{sel}"] = np.frombuffer(fn.read_bytes(), np.uint8)
         last = 1 if p.Npass2 > 0 else 0
         wsx = p.ws_x2 if last else p.ws_x1
         wsy = p.ws_y2 if last else p.ws_y1

@@ -151,6 +151,78 @@ def test_tecplot_writer_matches_oracle_and_sample_format(tmp_path):
         assert len(lines[3].split("\t")) == (10 if raw else 4)
 
 
+@pytest.mark.parametrize("case,sels", [("c0", (0, 1)), ("multigrid", (0, 1, 2, 3))])
+def test_tecplot_writer_byte_identical_to_reference_files(tmp_path, case, sels):
+    """write_vec_data_general's own output (recorded in the golden fixtures) reproduced
+    from the same arrays by piv_tecplot_write_arrays."""
+    gold = ROOT / "tests" / "golden" / f"golden_{case}.npz"
+    z = np.load(gold)
+    if "tecplot_sel0" not in z.files:
+        pytest.skip("fixture predates the Tecplot recordings")
+    import ast
+
+    pk = ast.literal_eval(str(z["params"][0]))
+    p = P.default_params(**pk)
+    g = P.geometry(p)
+    for sel in sels:
+        k = sel // 2
+        raw = sel % 2 == 0
+        dx = z[f"raw{k}_dx"] if raw else z[f"filt{k}_dx"]
+        dy = z[f"raw{k}_dy"] if raw else z[f"filt{k}_dy"]
+        dx = np.ascontiguousarray(dx, np.float32).ravel()
+        dy = np.ascontiguousarray(dy, np.float32).ravel()
+        out = tmp_path / f"{case}_{sel}.dat"
+        spx, spy = (p.spacing_x2, p.spacing_y2) if k else (p.spacing_x1, p.spacing_y1)
+        rc = P.lib().piv_tecplot_write_arrays(str(out).encode(), g["Nx_vec"][k], g["Ny_vec"][k], spx, spy,
+                                              int(raw), p.Npeak_save, dx.ctypes.data_as(P._F),
+                                              dy.ctypes.data_as(P._F))
+        assert rc == 0
+        assert out.read_bytes() == z[f"tecplot_sel{sel}"].tobytes(), f"selection {sel}"
+
+
+def test_tiff_roundtrip_and_big_endian(tmp_path):
+    import ctypes as C
+    import struct
+
+    rng = np.random.default_rng(2)
+    img = rng.integers(0, 256, (37, 53), dtype=np.uint8)
+    f = tmp_path / "a.tif"
+    assert P.lib().piv_tiff_write8(str(f).encode(), img.ctypes.data_as(P._U8), 53, 37) == 0
+    nx, ny, bits = C.c_int(), C.c_int(), C.c_int()
+    assert P.lib().piv_tiff_info(str(f).encode(), C.byref(nx), C.byref(ny), C.byref(bits)) == 0
+    assert (nx.value, ny.value, bits.value) == (53, 37, 8)
+    out = np.empty_like(img)
+    assert P.lib().piv_tiff_read8(str(f).encode(), out.ctypes.data_as(P._U8), 53, 37) == 0
+    assert np.array_equal(out, img)
+    # wrong size -> PIV_ERR_ARG
+    assert P.lib().piv_tiff_read8(str(f).encode(), out.ctypes.data_as(P._U8), 52, 37) == P.PIV_ERR_ARG
+    # a big-endian file with two strips and SHORT-typed dimensions
+    data = img.tobytes()
+    half = 19 * 53
+    entries = [(256, 3, 1, 53), (257, 3, 1, 37), (258, 3, 1, 8), (259, 3, 1, 1), (277, 3, 1, 1),
+               (278, 3, 1, 19), (273, 4, 2, None), (279, 4, 2, None)]
+    ifd = 8
+    hdr_len = ifd + 2 + 12 * len(entries) + 4
+    arrays = hdr_len
+    strips = arrays + 16
+    b = bytearray(b"MM" + struct.pack(">HI", 42, ifd) + struct.pack(">H", len(entries)))
+    for tag, typ, cnt, val in entries:
+        if tag == 273:
+            b += struct.pack(">HHII", tag, typ, cnt, arrays)
+        elif tag == 279:
+            b += struct.pack(">HHII", tag, typ, cnt, arrays + 8)
+        else:
+            b += struct.pack(">HHIHH", tag, typ, cnt, val, 0)
+    b += struct.pack(">I", 0)
+    b += struct.pack(">II", strips, strips + half) + struct.pack(">II", half, len(data) - half)
+    b += data
+    g = tmp_path / "be.tif"
+    g.write_bytes(bytes(b))
+    out[:] = 0
+    assert P.lib().piv_tiff_read8(str(g).encode(), out.ctypes.data_as(P._U8), 53, 37) == 0
+    assert np.array_equal(out, img)
+
+
 def test_synth_pair_deterministic_and_seeded():
     s = P.synth_params(96, 64, ppp=0.05, field=P.PIV_FIELD_UNIFORM, a=3.3, b=-1.7, seed=9)
     a1, a2 = P.synth_pair(s)

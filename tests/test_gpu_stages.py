@@ -136,7 +136,11 @@ def test_deformation(cuda, ws, sp):
         got = e.deformed(0)
     want, oob = O.deform(f2, op, g, 0, fx, fy)
     assert oob == 0
-    assert np.abs(got - want).max() < 2e-3
+    # the engine's FP32 bilinear sums contract into FMAs (as the reference's nvcc build
+    # does); the oracle rounds every product: a few ulp of the sample position times the
+    # image gradient (up to ~250 grey levels / px)
+    d = np.abs(got - want)
+    assert d.max() < 1e-2 and d.mean() < 1e-4
 
 
 def test_upsampling(cuda):
