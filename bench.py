@@ -246,6 +246,8 @@ def run_ours(args, rank, world, local):
                 "kernel_ms": round(kms, 4), "algorithmic_flops_per_launch": flops,
                 "peak_source": "FP32 FMA peak measured live on this GPU by piv_probe_fp32_peak"}
     launches = e.launches_per_pair() * args.steps
+    tuned = {f"grid{k + 1}": dict(zip(("windows_per_cta", "threads_per_cta", "tuned_ms"), e.xcorr_config(k)))
+             for k in range(2)}
     out = {
         "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(total_s * 1e3 / args.steps, 3), "higher_is_better": True,
@@ -253,7 +255,7 @@ def run_ours(args, rank, world, local):
         "data": "synthetic (seeded particle images, Lamb-Oseen vortex + shear)",
         "config": {"workload": "6600x4400 pair, MHE 40/0.91, grid 64x64@32 x2 -> 32x32@16 x3",
                    "vectors_per_pair": nvec, "pairs_per_step_per_gpu": 1, "parallelism": f"replicas x{world}",
-                   "l2": "flushed (512 MB write) before every timed step"},
+                   "l2": "flushed (512 MB write) before every timed step", "xcorr_autotune": tuned},
         "e2e": e2e, "roofline": roofline, "gpu_launches": launches, "clocks": clk.summary(),
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -64,6 +64,7 @@ def lib():
         h.ref_destroy.restype = None
         h.ref_mhe.argtypes = [_P, _U8P, _U8P]
         h.ref_run_pair.argtypes = [_P, _U8P, _U8P]
+        h.ref_run_pair_recording.argtypes = [_P, _U8P, _U8P, _FP, _FP, _FP, _FP]
         h.ref_median_only.argtypes = [_P]
         h.ref_get_raw.argtypes = [_P, C.c_int, _FP, _FP, _U8P]
         h.ref_get_filtered.argtypes = [_P, C.c_int, _FP, _FP, _U8P]
@@ -114,6 +115,18 @@ class RefEngine:
         rc = lib().ref_run_pair(self.h, _p(f1, C.c_uint8), _p(f2, C.c_uint8))
         if rc:
             raise RuntimeError(f"reference pair failed ({rc})")
+
+    def run_pair_recording(self, f1, f2, nt1, nt2):
+        """run_pair that also returns the filtered field each grid's last pass starts from."""
+        f1 = np.ascontiguousarray(f1, np.uint8)
+        f2 = np.ascontiguousarray(f2, np.uint8)
+        out = {k: np.zeros(n, np.float32) for k, n in (("p1x", nt1), ("p1y", nt1), ("p2x", nt2), ("p2y", nt2))}
+        rc = lib().ref_run_pair_recording(self.h, _p(f1, C.c_uint8), _p(f2, C.c_uint8),
+                                          _p(out["p1x"], C.c_float), _p(out["p1y"], C.c_float),
+                                          _p(out["p2x"], C.c_float), _p(out["p2y"], C.c_float))
+        if rc:
+            raise RuntimeError(f"reference pair failed ({rc})")
+        return out
 
     def median_only(self):
         rc = lib().ref_median_only(self.h)

@@ -101,9 +101,25 @@ int ref_mhe(ref_engine *e, const uint8_t *in, uint8_t *out)
     return cudaDeviceSynchronize() == cudaSuccess ? 0 : -4;
 }
 
+static void copy_field(float *dst, const float *src, int n)
+{
+    if (dst) cudaMemcpy(dst, src, (size_t)n * sizeof(float), cudaMemcpyDeviceToHost);
+}
+
 /* The per-pair body of X/main.cpp:263-326: frames into the engine's pinned buffers,
- * optional MHE round trip, prep, grid-1 and grid-2 pass loops. */
+ * optional MHE round trip, prep, grid-1 and grid-2 pass loops.  pred1x/y, pred2x/y
+ * (optional) receive the filtered field each grid's last pass starts from (its
+ * predictor and deformation field). */
+int ref_run_pair_recording(ref_engine *e, const uint8_t *f1, const uint8_t *f2, float *pred1x, float *pred1y,
+                           float *pred2x, float *pred2y);
+
 int ref_run_pair(ref_engine *e, const uint8_t *f1, const uint8_t *f2)
+{
+    return ref_run_pair_recording(e, f1, f2, nullptr, nullptr, nullptr, nullptr);
+}
+
+int ref_run_pair_recording(ref_engine *e, const uint8_t *f1, const uint8_t *f2, float *pred1x, float *pred1y,
+                           float *pred2x, float *pred2y)
 {
     xcorr2d_multi &x = e->x;
     size_t n = (size_t)e->p.Nx * e->p.Ny;
@@ -120,6 +136,10 @@ int ref_run_pair(ref_engine *e, const uint8_t *f1, const uint8_t *f2)
     x.prep_img_data();
     for (int j = 0; j < x.Npass1; j++) {
         if (j > 0) x.extend_filtered_vecfield_p1();
+        if (j == x.Npass1 - 1 && j > 0) {
+            copy_field(pred1x, x.d_disp_x_filter_p1, x.Nt1_vec);
+            copy_field(pred1y, x.d_disp_y_filter_p1, x.Nt1_vec);
+        }
         if (!x.Calc_cc_map_p1(j)) return -4;
         if (!x.MedianFilter_Smoothing_p1(e->p.Npass1_median, e->p.minNneigh_p1, e->p.residual_threshold_p1,
                                          e->p.insert_threshold_p1, e->p.Npass1_smooth))
@@ -130,6 +150,10 @@ int ref_run_pair(ref_engine *e, const uint8_t *f1, const uint8_t *f2)
         if (!x.Upsampling_vector_field()) return -4;
         for (int j = 0; j < x.Npass2; j++) {
             x.extend_filtered_vecfield_p2();
+            if (j == x.Npass2 - 1) {
+                copy_field(pred2x, x.d_disp_x_filter_p2, x.Nt2_vec);
+                copy_field(pred2y, x.d_disp_y_filter_p2, x.Nt2_vec);
+            }
             if (!x.Calc_cc_map_p2()) return -4;
             if (!x.MedianFilter_Smoothing_p2(e->p.Npass2_median, e->p.minNneigh_p2, e->p.residual_threshold_p2,
                                              e->p.insert_threshold_p2, e->p.Npass2_smooth, 1))

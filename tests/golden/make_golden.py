@@ -72,7 +72,12 @@ def make_case(name, sk, pk, outdir):
         if p.if_mhe:
             out["f1_mhe"] = r.mhe(f1)
             out["f2_mhe"] = r.mhe(f2)
-        r.run_pair(f1, f2)
+        pred = r.run_pair_recording(f1, f2, g["Nt_vec"][0], g["Nt_vec"][1])
+        # the filtered field each grid's last pass started from (predictor + deformation field)
+        if p.Npass1 > 1:
+            out["pred0_dx"], out["pred0_dy"] = pred["p1x"], pred["p1y"]
+        if p.Npass2 > 0:
+            out["pred1_dx"], out["pred1_dy"] = pred["p2x"], pred["p2y"]
         for k in range(2 if p.Npass2 > 0 else 1):
             nt = g["Nt_vec"][k]
             dx, dy, v = r.raw(k, nt)

@@ -65,7 +65,8 @@ def test_driver_error_paths(cuda, tmp_path):
     r = subprocess.run([str(EXE), str(tmp_path / "nope.dat")], capture_output=True, text=True, timeout=60)
     assert r.returncode == 1 and "Can't open parameter file!" in r.stdout
     par = write_setup(tmp_path, [3])
-    lines = par.read_text().split("\r\n")
+    lines = par.read_bytes().decode().split("\r\n")
+    assert len(lines) == 50
     (tmp_path / "short.dat").write_text("\n".join(lines[:41]))
     r = subprocess.run([str(EXE), str(tmp_path / "short.dat")], capture_output=True, text=True, timeout=60)
     assert r.returncode == 1 and "Parameter missing" in r.stdout
