@@ -58,35 +58,40 @@ def near_ties(planes, bx, by, nps, rel=1e-5):
 def fit_tolerance(planes, idx, wsx, rel_cc=1e-5):
     """Per-candidate bound on |engine - reference| for the 3-point Gaussian fit.
 
-    delta = num / (2 den), num = ln f- - ln f+, den = ln f- + ln f+ - 2 ln f0.  The
-    reference forms den in FP32 (each logf within 1 ulp, then two roundings) and its
-    cuFFT planes differ from the engine's by up to rel_cc; the engine forms den in FP64.
-    Propagating those errors: |d delta| <= (|delta| * e_den + e_num / 2) / |den| with
-    e_num = 2 rel_cc + 2^-23 (|ln f-| + |ln f+|), e_den = 4 rel_cc + 2^-22 (|ln f-| + |ln f+| + 2|ln f0|).
-    Well-conditioned peaks get ~1e-3 px; flat peaks (den -> 0) are where the reference's
-    FP32 cancellation dominates."""
+    delta = num / (2 den), num = ln f- - ln f+, den = ln f- + ln f+ - 2 ln f0.  Two FP32
+    FFTs of different algorithms agree to an ABSOLUTE error of about rel_cc times the
+    window's largest correlation value (the planes test asserts it), so a value c carries
+    a log error of rel_cc * max / c -- large for weak secondary peaks.  The reference also
+    forms den in FP32 (each logf within 1 ulp, then two roundings); the engine in FP64.
+    Propagating: |d delta| <= (|delta| * e_den + e_num / 2) / |den| with
+    e_num = e(f-) + e(f+) + 2^-23 (|ln f-| + |ln f+|),
+    e_den = e(f-) + e(f+) + 2 e(f0) + 2^-22 (|ln f-| + |ln f+| + 2 |ln f0|).
+    Strong, well-conditioned peaks get ~1e-3 px."""
     n, wsy, _ = planes.shape
     tols = []
     for axis in (1, wsx):
         t = np.full(idx.shape, 1e-3)
         for w in range(n):
             flat = planes[w].ravel()
+            cmax = float(flat.max())
             for q in range(idx.shape[1]):
                 li = idx[w, q]
                 if li < 0 or li - axis < 0 or li + axis >= flat.size:
                     continue
                 c0, c1, c2 = (float(flat[li - axis]), float(flat[li]), float(flat[li + axis]))
                 if min(c0, c1, c2) <= 0:
+                    t[w, q] = np.inf
                     continue
                 f0, f1, f2 = np.log(c0), np.log(c1), np.log(c2)
                 den = f0 + f2 - 2 * f1
-                if den == 0:
-                    t[w, q] = np.inf
+                e0, e1, e2 = (rel_cc * cmax / c0, rel_cc * cmax / c1, rel_cc * cmax / c2)
+                e_num = e0 + e2 + 2.0 ** -23 * (abs(f0) + abs(f2))
+                e_den = e0 + e2 + 2 * e1 + 2.0 ** -22 * (abs(f0) + abs(f2) + 2 * abs(f1))
+                if abs(den) <= e_den:
+                    t[w, q] = np.inf  # the denominator's sign is not determined at this precision
                     continue
                 delta = (f0 - f2) / den / 2
-                e_num = 2 * rel_cc + 2.0 ** -23 * (abs(f0) + abs(f2))
-                e_den = 4 * rel_cc + 2.0 ** -22 * (abs(f0) + abs(f2) + 2 * abs(f1))
-                t[w, q] = 1e-3 + (abs(delta) * e_den + e_num / 2) / abs(den)
+                t[w, q] = 1e-3 + (abs(delta) * e_den + e_num / 2) / (abs(den) - e_den)
         tols.append(t)
     return tols
 
@@ -168,7 +173,10 @@ def test_peaks_and_candidates(run):
         tx, ty = fit_tolerance(planes, idx, p.ws_x2 if k else p.ws_x1)
         assert (np.abs(dx - z[f"raw{k}_dx"])[both] <= tx[both]).all()
         assert (np.abs(dy - z[f"raw{k}_dy"])[both] <= ty[both]).all()
-        assert (np.abs(dx - z[f"raw{k}_dx"])[both] < 1e-3).mean() >= 0.999
+        # the main peak of each window: within 1e-3 px almost everywhere
+        b0 = both[:, 0]
+        d0 = np.maximum(np.abs(dx - z[f"raw{k}_dx"]), np.abs(dy - z[f"raw{k}_dy"]))[:, 0]
+        assert (d0[b0] < 1e-3).mean() >= 0.999
         assert np.abs(val[same] - z[f"peaks{k}_value"][same]).max() <= 1e-5 * np.abs(val).max()
 
 
