@@ -138,6 +138,7 @@ EXPORTS = {
     "piv_mhe_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_float, C.POINTER(_P)]),
     "piv_mhe_process": (C.c_int, [_P, _P, _P, _P]),
     "piv_mhe_destroy": (C.c_int, [_P]),
+    "piv_mhe_process_noalloc": (C.c_int, [_P, _P, C.c_int, C.c_int, C.c_int, C.c_float, _P]),
     "piv_synth_pair": (C.c_int, [C.POINTER(PivSynthParams), _U8, _U8]),
     "piv_synth_field": (C.c_int, [C.POINTER(PivSynthParams), _F, _F, C.c_int, _F, _F]),
 }
