@@ -24,34 +24,58 @@ __device__ __forceinline__ float ext_field(const float *f, int Nx, int Ny, int m
 // written exactly as the reference writes it.  Frame-2 taps outside the padded
 // frame read 0 (the reference reads its zero padding there, or out of bounds).
 // ------------------------------------------------------------------------------
+// One output pixel of Kernel_Window_Deformation_2d given the 8 field values of its cell.
+__device__ __forceinline__ float deform_pixel(const DeformArgs &a, int idx, int Y, float a_x, float a_y, float u1,
+                                              float u2, float u3, float u4, float v1, float v2, float v3, float v4,
+                                              int col_off, int row_off)
+{
+    float ce1 = (1 - a_x) * (1 - a_y);
+    float ce2 = a_x * (1 - a_y);
+    float ce3 = (1 - a_x) * a_y;
+    float ce4 = a_x * a_y;
+    a_x = (float)idx + ce1 * u1 + ce2 * u2 + ce3 * u3 + ce4 * u4;
+    a_y = (float)Y + ce1 * v1 + ce2 * v2 + ce3 * v3 + ce4 * v4;
+    int i_x = (int)floorf(a_x);
+    int i_y = (int)floorf(a_y);
+    a_x = a_x - (float)i_x;
+    a_y = a_y - (float)i_y;
+    // aug_ex column i_x + hfws_x holds image column i_x - Nx_left -> padded-frame column
+    const int c0 = i_x + col_off, r0 = i_y + row_off;
+    float p[4];
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+        const int c = c0 + (t & 1), r = r0 + (t >> 1);
+        p[t] = (c >= 0 && c < a.f2.cols && r >= 0 && r < a.f2.rows)
+                   ? (float)__ldg(a.f2.base + (size_t)r * a.f2.pitch + c)
+                   : 0.f;
+    }
+    ce1 = (1 - a_x) * (1 - a_y);
+    ce2 = a_x * (1 - a_y);
+    ce3 = (1 - a_x) * a_y;
+    ce4 = a_x * a_y;
+    return ce1 * p[0] + ce2 * p[1] + ce3 * p[2] + ce4 * p[3];
+}
+
+// Each thread writes 8 consecutive pixels of one row (two float4 stores).  When the
+// vector spacing and the field origin are multiples of 8 (the `cell8` launches), the 8
+// pixels lie in one cell of the field, so its 8 values are loaded once.
+template <bool CELL8>
 __global__ void __launch_bounds__(256) deform_kernel(const DeformArgs a)
 {
-    const int X0 = (blockIdx.x * blockDim.x + threadIdx.x) * 4;
+    const int X0 = (blockIdx.x * blockDim.x + threadIdx.x) * 8;
     const int Y = blockIdx.y;
     if (X0 >= a.Nx_aug || Y >= a.Ny_aug) return;
     const float x_st_vec = (float)(a.hfws_x - a.sp_x * 3), y_st_vec = (float)(a.hfws_y - a.sp_y * 3);
     const float vsx = (float)a.sp_x, vsy = (float)a.sp_y;
-    const int x_st_inten = -a.hfws_x, y_st_inten = -a.hfws_y;
-    // aug_ex column c holds image column c - (Nx_left + hfws_x) -> padded-frame column
-    const int col_off = a.f2.mx - a.Nx_left - a.hfws_x, row_off = a.f2.my - a.Ny_left - a.hfws_y;
+    const int col_off = a.f2.mx - a.Nx_left, row_off = a.f2.my - a.Ny_left;
 
-    float a_y0 = ((float)Y - y_st_vec) / vsy;
-    const int i_y0 = (int)floorf(a_y0);
-    a_y0 = a_y0 - (float)i_y0;
+    float a_y = ((float)Y - y_st_vec) / vsy;
+    const int i_y = (int)floorf(a_y);
+    a_y = a_y - (float)i_y;
 
-    float res[4];
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        const int idx = X0 + q;
-        float a_x = ((float)idx - x_st_vec) / vsx;
-        float a_y = a_y0;
-        int i_x = (int)floorf(a_x);
-        int i_y = i_y0;
-        a_x = a_x - (float)i_x;
-        float ce1 = (1 - a_x) * (1 - a_y);
-        float ce2 = a_x * (1 - a_y);
-        float ce3 = (1 - a_x) * a_y;
-        float ce4 = a_x * a_y;
+    float res[8];
+    if (CELL8) {
+        const int i_x = (int)floorf(((float)X0 - x_st_vec) / vsx);
         const float u1 = ext_field(a.fx, a.Nx_vec, a.Ny_vec, i_x, i_y);
         const float u2 = ext_field(a.fx, a.Nx_vec, a.Ny_vec, i_x + 1, i_y);
         const float u3 = ext_field(a.fx, a.Nx_vec, a.Ny_vec, i_x, i_y + 1);
@@ -60,41 +84,50 @@ __global__ void __launch_bounds__(256) deform_kernel(const DeformArgs a)
         const float v2 = ext_field(a.fy, a.Nx_vec, a.Ny_vec, i_x + 1, i_y);
         const float v3 = ext_field(a.fy, a.Nx_vec, a.Ny_vec, i_x, i_y + 1);
         const float v4 = ext_field(a.fy, a.Nx_vec, a.Ny_vec, i_x + 1, i_y + 1);
-        a_x = (float)idx + ce1 * u1 + ce2 * u2 + ce3 * u3 + ce4 * u4;
-        a_y = (float)Y + ce1 * v1 + ce2 * v2 + ce3 * v3 + ce4 * v4;
-
-        i_x = (int)floorf(a_x);
-        i_y = (int)floorf(a_y);
-        a_x = a_x - (float)i_x;
-        a_y = a_y - (float)i_y;
-        i_x = i_x - x_st_inten;  // aug_ex column
-        i_y = i_y - y_st_inten;  // aug_ex row
-        const int c0 = i_x + col_off, r0 = i_y + row_off;
-        auto tap = [&](int c, int r) -> float {
-            return (c >= 0 && c < a.f2.cols && r >= 0 && r < a.f2.rows)
-                       ? (float)__ldg(a.f2.base + (size_t)r * a.f2.pitch + c)
-                       : 0.f;
-        };
-        const float p1 = tap(c0, r0), p2 = tap(c0 + 1, r0), p3 = tap(c0, r0 + 1), p4 = tap(c0 + 1, r0 + 1);
-        ce1 = (1 - a_x) * (1 - a_y);
-        ce2 = a_x * (1 - a_y);
-        ce3 = (1 - a_x) * a_y;
-        ce4 = a_x * a_y;
-        res[q] = ce1 * p1 + ce2 * p2 + ce3 * p3 + ce4 * p4;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const int idx = X0 + q;
+            float a_x = ((float)idx - x_st_vec) / vsx;
+            a_x = a_x - (float)i_x;
+            res[q] = deform_pixel(a, idx, Y, a_x, a_y, u1, u2, u3, u4, v1, v2, v3, v4, col_off, row_off);
+        }
+    } else {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const int idx = X0 + q;
+            float a_x = ((float)idx - x_st_vec) / vsx;
+            const int i_x = (int)floorf(a_x);
+            a_x = a_x - (float)i_x;
+            res[q] = deform_pixel(a, idx, Y, a_x, a_y, ext_field(a.fx, a.Nx_vec, a.Ny_vec, i_x, i_y),
+                                  ext_field(a.fx, a.Nx_vec, a.Ny_vec, i_x + 1, i_y),
+                                  ext_field(a.fx, a.Nx_vec, a.Ny_vec, i_x, i_y + 1),
+                                  ext_field(a.fx, a.Nx_vec, a.Ny_vec, i_x + 1, i_y + 1),
+                                  ext_field(a.fy, a.Nx_vec, a.Ny_vec, i_x, i_y),
+                                  ext_field(a.fy, a.Nx_vec, a.Ny_vec, i_x + 1, i_y),
+                                  ext_field(a.fy, a.Nx_vec, a.Ny_vec, i_x, i_y + 1),
+                                  ext_field(a.fy, a.Nx_vec, a.Ny_vec, i_x + 1, i_y + 1), col_off, row_off);
+        }
     }
     float *dst = a.out + (size_t)Y * a.out_pitch + X0;
-    if (X0 + 3 < a.Nx_aug) {
-        *reinterpret_cast<float4 *>(dst) = make_float4(res[0], res[1], res[2], res[3]);
+    if (X0 + 7 < a.Nx_aug) {
+        reinterpret_cast<float4 *>(dst)[0] = make_float4(res[0], res[1], res[2], res[3]);
+        reinterpret_cast<float4 *>(dst)[1] = make_float4(res[4], res[5], res[6], res[7]);
     } else {
-        for (int q = 0; q < 4 && X0 + q < a.Nx_aug; ++q) dst[q] = res[q];
+        for (int q = 0; q < 8 && X0 + q < a.Nx_aug; ++q) dst[q] = res[q];
     }
 }
 
 cudaError_t launch_deform(const DeformArgs &a, cudaStream_t s)
 {
     dim3 block(256);
-    dim3 grid(((a.Nx_aug + 3) / 4 + 255) / 256, a.Ny_aug);
-    deform_kernel<<<grid, block, 0, s>>>(a);
+    dim3 grid(((a.Nx_aug + 7) / 8 + 255) / 256, a.Ny_aug);
+    // the 8-pixel runs X0..X0+7 (X0 % 8 == 0) share a field cell when the cell edges
+    // x_st + m*sp are multiples of 8; the cell index is then exact for every pixel of
+    // the run (its float quotient is exact for these small integers)
+    const int x_st = a.hfws_x - a.sp_x * 3;
+    const bool cell8 = (a.sp_x % 8 == 0) && (((x_st % 8) + 8) % 8 == 0);
+    if (cell8) deform_kernel<true><<<grid, block, 0, s>>>(a);
+    else deform_kernel<false><<<grid, block, 0, s>>>(a);
     return cudaGetLastError();
 }
 
@@ -193,6 +226,60 @@ __device__ float median_bubble(float *d, int n, int stride)
     return d[((n - 1) / 2) * stride];
 }
 
+// Ascending bitonic sort of a register array (N a power of two, all indices compile-time).
+template <int N, int K, int J>
+__device__ __forceinline__ void bitonic_step(float (&a)[N])
+{
+    static_for<0, N>([&](auto ic) {
+        constexpr int i = decltype(ic)::value, l = i ^ J;
+        if constexpr (l > i) {
+            const float x = a[i], y = a[l];
+            if constexpr ((i & K) == 0) {
+                a[i] = fminf(x, y);
+                a[l] = fmaxf(x, y);
+            } else {
+                a[i] = fmaxf(x, y);
+                a[l] = fminf(x, y);
+            }
+        }
+    });
+    if constexpr (J > 1) bitonic_step<N, K, J / 2>(a);
+}
+
+template <int N, int K = 2>
+__device__ __forceinline__ void bitonic_sort(float (&a)[N])
+{
+    bitonic_step<N, K, K / 2>(a);
+    if constexpr (K < N) bitonic_sort<N, K * 2>(a);
+}
+
+// Median of the first n (<= N) entries of a sorted array, as Calc_median defines it
+// (mean of the two middle values for even n, FP32).
+// a[idx] for a runtime idx by a binary select tree over compile-time indices (keeps the
+// array in registers; a compare-and-select loop is turned back into a local-memory load).
+template <int N>
+__device__ __forceinline__ float select_dyn(const float (&a)[N], int idx)
+{
+    if constexpr (N == 1) {
+        return a[0];
+    } else {
+        float t[N / 2];
+        const bool up = (idx & (N / 2)) != 0;
+#pragma unroll
+        for (int i = 0; i < N / 2; ++i) t[i] = up ? a[i + N / 2] : a[i];
+        return select_dyn<N / 2>(t, idx);
+    }
+}
+
+template <int N>
+__device__ __forceinline__ float median_sorted(const float (&a)[N], int n)
+{
+    const float hi = select_dyn<N>(a, n / 2);  // n odd: (n-1)/2 == n/2
+    if (n % 2 != 0) return hi;
+    const float lo = select_dyn<N>(a, n / 2 - 1);
+    return (hi + lo) / 2;
+}
+
 struct MedianPass {
     const float *cdx, *cdy;
     const uint8_t *cvalid;
@@ -212,6 +299,47 @@ struct MedianPass {
 // thread per vector.  Neighbours are gathered in raster stencil order with the centre
 // slot (wx*wy-1)/2 skipped; the medians are order statistics, so the gather order
 // does not change them.
+__device__ __forceinline__ void median_neighbour(const MedianPass &a, int id, bool &ok, float &fxv, float &fyv)
+{
+    if (a.ix) {
+        ok = a.iv[id] != 0;
+        fxv = a.ix[id];
+        fyv = a.iy[id];
+    } else {
+        ok = a.cvalid[(size_t)id * a.Nps] != 0;
+        fxv = a.cdx[(size_t)id * a.Nps];
+        fyv = a.cdy[(size_t)id * a.Nps];
+    }
+}
+
+// median_filtering's decision: the first valid candidate whose normalised residuals are
+// both below the insert threshold replaces the vector, else (0, 0, invalid).
+__device__ __forceinline__ void median_decide(const MedianPass &a, int v, float mx, float my, float dmx, float dmy,
+                                              float &rx, float &ry, uint8_t &rv)
+{
+    const float epsilon = 0.1f;  // X/xcorr2d_multi_grid.cuh:192
+    for (int i = 0; i < a.Nps; ++i) {
+        const size_t c = (size_t)v * a.Nps + i;
+        if (!a.cvalid[c]) continue;
+        const float cx = a.cdx[c], cy = a.cdy[c];
+        const float devix = __fdiv_rn(fabsf(cx - mx), dmx + epsilon);
+        const float deviy = __fdiv_rn(fabsf(cy - my), dmy + epsilon);
+        if (devix < a.thr && deviy < a.thr) {
+            rv = 1;
+            rx = cx;
+            ry = cy;
+            return;
+        }
+    }
+}
+
+// One pass of organize_median_filter_data + median_validity + Calc_median x4 +
+// Calc_devi x2 + median_filtering (X/xcorr2d_multi_grid.cu:209-296, 1464-1513), one
+// thread per vector.  The medians are order statistics, so how they are found does not
+// change them: REG (stencils of at most 32 cells) keeps one register slot per stencil
+// cell (+inf when the neighbour is absent) and sorts with a bitonic network; larger
+// stencils use the reference's partial bubble sort on a thread-private shared slice.
+template <bool REG>
 __global__ void __launch_bounds__(128) median_pass_kernel(const MedianPass a)
 {
     extern __shared__ float sl[];
@@ -219,10 +347,6 @@ __global__ void __launch_bounds__(128) median_pass_kernel(const MedianPass a)
     const int Nt = a.Nx * a.Ny;
     if (v >= Nt) return;
     const int Ntm = a.wx * a.wy;
-    // thread-private slices interleaved across threads: element k of thread t at k*blockDim + t
-    const int stride = blockDim.x;
-    float *xs = sl + threadIdx.x, *ys = sl + (size_t)Ntm * blockDim.x + threadIdx.x;
-    const float epsilon = 0.1f;  // X/xcorr2d_multi_grid.cuh:192
     float rx = 0.f, ry = 0.f;
     uint8_t rv = 0;
     if (!a.median) {
@@ -232,50 +356,66 @@ __global__ void __launch_bounds__(128) median_pass_kernel(const MedianPass a)
     } else {
         const int vy = v / a.Nx, vx = v - vy * a.Nx;
         const int hfwx = (a.wx - 1) / 2, hfwy = (a.wy - 1) / 2;
-        int n = 0;
-        for (int t = 0; t < Ntm; ++t) {
-            if (t == (Ntm - 1) / 2) continue;
-            const int ty = t / a.wx, tx = t - ty * a.wx;
-            const int x = vx - hfwx + tx, y = vy - hfwy + ty;
-            if (x >= 0 && x <= a.Nx - 1 && y >= 0 && y <= a.Ny - 1) {
-                const int id = y * a.Nx + x;
+        const int centre = (Ntm - 1) / 2;
+        if constexpr (REG) {
+            const float inf = __int_as_float(0x7f800000);
+            float xs[32], ys[32];
+            int n = 0;
+#pragma unroll
+            for (int t = 0; t < 32; ++t) {
+                const int ty = t / a.wx, tx = t - ty * a.wx;
+                const int x = vx - hfwx + tx, y = vy - hfwy + ty;
+                const bool inb = (t < Ntm) & (t != centre) & (x >= 0) & (x <= a.Nx - 1) & (y >= 0) & (y <= a.Ny - 1);
                 bool ok;
-                float fxv, fyv;
-                if (a.ix) {
-                    ok = a.iv[id] != 0;
-                    fxv = a.ix[id];
-                    fyv = a.iy[id];
-                } else {
-                    ok = a.cvalid[(size_t)id * a.Nps] != 0;
-                    fxv = a.cdx[(size_t)id * a.Nps];
-                    fyv = a.cdy[(size_t)id * a.Nps];
+                float px, py;
+                median_neighbour(a, inb ? y * a.Nx + x : v, ok, px, py);  // always a valid address
+                ok = ok & inb;
+                xs[t] = ok ? px : inf;
+                ys[t] = ok ? py : inf;
+                n += ok;
+            }
+            if (n >= a.minN && n >= 1) {
+                bitonic_sort<32>(xs);
+                bitonic_sort<32>(ys);
+                const float mx = median_sorted<32>(xs, n), my = median_sorted<32>(ys, n);
+#pragma unroll
+                for (int q = 0; q < 32; ++q) {
+                    xs[q] = (q < n) ? fabsf(xs[q] - mx) : inf;
+                    ys[q] = (q < n) ? fabsf(ys[q] - my) : inf;
                 }
-                if (ok) {
-                    xs[n * stride] = fxv;
-                    ys[n * stride] = fyv;
-                    n++;
+                bitonic_sort<32>(xs);
+                bitonic_sort<32>(ys);
+                const float dmx = median_sorted<32>(xs, n), dmy = median_sorted<32>(ys, n);
+                median_decide(a, v, mx, my, dmx, dmy, rx, ry, rv);
+            }
+        } else {
+            // thread-private slices interleaved across threads: element k of thread t at k*blockDim + t
+            const int stride = blockDim.x;
+            float *xs = sl + threadIdx.x, *ys = sl + (size_t)Ntm * blockDim.x + threadIdx.x;
+            int n = 0;
+            for (int t = 0; t < Ntm; ++t) {
+                if (t == centre) continue;
+                const int ty = t / a.wx, tx = t - ty * a.wx;
+                const int x = vx - hfwx + tx, y = vy - hfwy + ty;
+                if (x >= 0 && x <= a.Nx - 1 && y >= 0 && y <= a.Ny - 1) {
+                    bool ok;
+                    float fxv, fyv;
+                    median_neighbour(a, y * a.Nx + x, ok, fxv, fyv);
+                    if (ok) {
+                        xs[n * stride] = fxv;
+                        ys[n * stride] = fyv;
+                        n++;
+                    }
                 }
             }
-        }
-        if (n >= a.minN && n >= 1) {
-            const float mx = median_bubble(xs, n, stride), my = median_bubble(ys, n, stride);
-            for (int q = 0; q < n; ++q) {
-                xs[q * stride] = fabsf(xs[q * stride] - mx);
-                ys[q * stride] = fabsf(ys[q * stride] - my);
-            }
-            const float dmx = median_bubble(xs, n, stride), dmy = median_bubble(ys, n, stride);
-            for (int i = 0; i < a.Nps; ++i) {
-                const size_t c = (size_t)v * a.Nps + i;
-                if (!a.cvalid[c]) continue;
-                const float cx = a.cdx[c], cy = a.cdy[c];
-                const float devix = __fdiv_rn(fabsf(cx - mx), dmx + epsilon);
-                const float deviy = __fdiv_rn(fabsf(cy - my), dmy + epsilon);
-                if (devix < a.thr && deviy < a.thr) {
-                    rv = 1;
-                    rx = cx;
-                    ry = cy;
-                    break;
+            if (n >= a.minN && n >= 1) {
+                const float mx = median_bubble(xs, n, stride), my = median_bubble(ys, n, stride);
+                for (int q = 0; q < n; ++q) {
+                    xs[q * stride] = fabsf(xs[q * stride] - mx);
+                    ys[q * stride] = fabsf(ys[q * stride] - my);
                 }
+                const float dmx = median_bubble(xs, n, stride), dmy = median_bubble(ys, n, stride);
+                median_decide(a, v, mx, my, dmx, dmy, rx, ry, rv);
             }
         }
     }
@@ -401,12 +541,17 @@ cudaError_t launch_validate(const ValidateArgs &a, cudaStream_t s)
         m.median = a.Npass_median > 0;
         m.list = (st == steps_med) ? list : nullptr;
         m.list_n = a.list_n;
-        const size_t smem = m.median ? (size_t)2 * a.wx_med * a.wy_med * tb * sizeof(float) : 0;
-        if (smem > 48 * 1024) {
-            e = cudaFuncSetAttribute(median_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            if (e != cudaSuccess) return e;
+        if (a.wx_med * a.wy_med <= 32) {
+            median_pass_kernel<true><<<(Nt + tb - 1) / tb, tb, 0, s>>>(m);
+        } else {
+            const size_t smem = m.median ? (size_t)2 * a.wx_med * a.wy_med * tb * sizeof(float) : 0;
+            if (smem > 48 * 1024) {
+                e = cudaFuncSetAttribute(median_pass_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+                if (e != cudaSuccess) return e;
+            }
+            median_pass_kernel<false><<<(Nt + tb - 1) / tb, tb, smem, s>>>(m);
         }
-        median_pass_kernel<<<(Nt + tb - 1) / tb, tb, smem, s>>>(m);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
         cx = m.ox;
         cy = m.oy;

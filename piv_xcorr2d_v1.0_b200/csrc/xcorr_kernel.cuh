@@ -36,6 +36,14 @@
 
 namespace piv {
 
+// Byte b of w as a float: the byte is placed into the low mantissa bits of 2^23
+// (0x4B0000bb), then 2^23 is subtracted -- exact for 0..255, one PRMT + one FADD.
+template <int b>
+__device__ __forceinline__ float byte_to_float(uint32_t w)
+{
+    return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7440u | b)) - 8388608.0f;
+}
+
 template <int WSX>
 __device__ __forceinline__ void load_u8_row(const uint8_t *p, float (&v)[WSX])
 {
@@ -45,11 +53,14 @@ __device__ __forceinline__ void load_u8_row(const uint8_t *p, float (&v)[WSX])
 #pragma unroll
             for (int q = 0; q < WSX / 8; ++q) {
                 uint2 u = __ldg(reinterpret_cast<const uint2 *>(p) + q);
-#pragma unroll
-                for (int b = 0; b < 4; ++b) {
-                    v[8 * q + b] = (float)((u.x >> (8 * b)) & 0xffu);
-                    v[8 * q + 4 + b] = (float)((u.y >> (8 * b)) & 0xffu);
-                }
+                v[8 * q + 0] = byte_to_float<0>(u.x);
+                v[8 * q + 1] = byte_to_float<1>(u.x);
+                v[8 * q + 2] = byte_to_float<2>(u.x);
+                v[8 * q + 3] = byte_to_float<3>(u.x);
+                v[8 * q + 4] = byte_to_float<0>(u.y);
+                v[8 * q + 5] = byte_to_float<1>(u.y);
+                v[8 * q + 6] = byte_to_float<2>(u.y);
+                v[8 * q + 7] = byte_to_float<3>(u.y);
             }
             return;
         }
@@ -58,8 +69,10 @@ __device__ __forceinline__ void load_u8_row(const uint8_t *p, float (&v)[WSX])
 #pragma unroll
         for (int q = 0; q < WSX / 4; ++q) {
             uint32_t u = __ldg(reinterpret_cast<const uint32_t *>(p) + q);
-#pragma unroll
-            for (int b = 0; b < 4; ++b) v[4 * q + b] = (float)((u >> (8 * b)) & 0xffu);
+            v[4 * q + 0] = byte_to_float<0>(u);
+            v[4 * q + 1] = byte_to_float<1>(u);
+            v[4 * q + 2] = byte_to_float<2>(u);
+            v[4 * q + 3] = byte_to_float<3>(u);
         }
         return;
     }
@@ -223,7 +236,7 @@ __global__ void __launch_bounds__(NT) xcorr_peak_kernel(const XcorrArgs a)
     // ---------------- P5: peaks, warp per window ----------------
     const int warp = tid >> 5, lane = tid & 31;
     constexpr int NW = NT / 32;
-    const int rows = WSY - 2 * g.by, cols = WSX - 2 * g.bx;
+    const int rows = WSY - 2 * g.by;
     for (int b = warp; b < B; b += NW) {
         const int w = w_base + b;
         if (w >= a.w_end) continue;
@@ -237,6 +250,7 @@ __global__ void __launch_bounds__(NT) xcorr_peak_kernel(const XcorrArgs a)
             }
             continue;
         }
+        // lane-local top-K of the lane's region rows, sorted (value desc, index asc)
         float tv[K];
         int ti[K];
 #pragma unroll
@@ -245,39 +259,55 @@ __global__ void __launch_bounds__(NT) xcorr_peak_kernel(const XcorrArgs a)
             ti[k] = INT_MAX;
         }
         int cnt = 0;
-        const int nreg = rows * cols;
-        for (int t = lane; t < nreg; t += 32) {
-            const int jj = t / cols, ii = t - jj * cols;
-            const int j = g.by + jj, i = g.bx + ii;
-            const float *pr = P + j * LDF + i;
-            const float v = pr[0];
-            if (v > 0.f && v >= pr[-1] && v >= pr[1] && v >= pr[-LDF] && v >= pr[LDF]) {
-                cnt++;
-                topk_insert<K>(tv, ti, v, j * WSX + i);
+        for (int jj = lane; jj < rows; jj += 32) {
+            const int j = g.by + jj;
+            const float *pm = P + j * LDF;
+            float mid[WSX];
+#pragma unroll
+            for (int i = 0; i < WSX; ++i) mid[i] = pm[i];
+#pragma unroll
+            for (int i = 1; i < WSX - 1; ++i) {
+                const float v = mid[i];
+                // branch-free local-maximum test (bitwise &, no short circuit)
+                const bool c = (i >= g.bx) & (i <= WSX - 1 - g.bx) & (v > 0.f) & (v >= mid[i - 1]) &
+                               (v >= mid[i + 1]) & (v >= pm[i - LDF]) & (v >= pm[i + LDF]);
+                cnt += c;
+                if (c && better(v, j * WSX + i, tv[K - 1], ti[K - 1])) topk_insert<K>(tv, ti, v, j * WSX + i);
             }
         }
 #pragma unroll
-        for (int off = 16; off >= 1; off >>= 1) {
-            cnt += __shfl_xor_sync(0xffffffffu, cnt, off);
-            float pv[K];
-            int pi[K];
+        for (int off = 16; off >= 1; off >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, off);
+        // the window's top Nps: Nps rounds of a warp arg-max over the lanes' list heads;
+        // indices are unique, so exactly one lane owns each winner and pops it
+        float v = -1.f;
+        int idx = INT_MAX;
+        for (int k = 0; k < g.Nps; ++k) {
+            float bv = tv[0];
+            int bi = ti[0];
 #pragma unroll
-            for (int k = 0; k < K; ++k) {
-                pv[k] = __shfl_xor_sync(0xffffffffu, tv[k], off);
-                pi[k] = __shfl_xor_sync(0xffffffffu, ti[k], off);
+            for (int off = 16; off >= 1; off >>= 1) {
+                const float ov = __shfl_xor_sync(0xffffffffu, bv, off);
+                const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
+                if (better(ov, oi, bv, bi)) {
+                    bv = ov;
+                    bi = oi;
+                }
             }
+            if (lane == k) {
+                v = bv;
+                idx = bi;
+            }
+            if (bi == ti[0] && bv > 0.f) {
 #pragma unroll
-            for (int k = 0; k < K; ++k) topk_insert<K>(tv, ti, pv[k], pi[k]);
+                for (int s = 0; s < K - 1; ++s) {
+                    tv[s] = tv[s + 1];
+                    ti[s] = ti[s + 1];
+                }
+                tv[K - 1] = -1.f;
+                ti[K - 1] = INT_MAX;
+            }
         }
         if (lane < g.Nps) {
-            float v = -1.f;
-            int idx = INT_MAX;
-#pragma unroll
-            for (int k = 0; k < K; ++k)
-                if (k == lane) {
-                    v = tv[k];
-                    idx = ti[k];
-                }
             float ox = 0.f, oy = 0.f;
             bool ok = false;
             if (v > 0.f) {
