@@ -146,38 +146,11 @@ def cpu_baseline(P, f1, f2, rows):
                       f"({nvec} grid-2 vectors in {dt:.2f} s)"}
 
 
-def dist_setup(n_gpus):
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        import datetime
+def replicas():
+    load_pkg()
+    import piv_b200.replicas as R
 
-        import torch
-        import torch.distributed as dist
-
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
-                                device_id=torch.device("cuda", local))
-    return rank, world, local
-
-
-def dist_max(x, world):
-    if world == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
-
-
-def dist_barrier(world):
-    if world > 1:
-        import torch.distributed as dist
-
-        dist.barrier()
+    return R
 
 
 def run_ours(args, rank, world, local):
@@ -197,9 +170,10 @@ def run_ours(args, rank, world, local):
     for _ in range(args.warmup):
         e.run_pair()
         e.synchronize()
+    R = replicas()
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    dist_barrier(world)
+    R.barrier(world)
     torch.cuda.synchronize()
     h1, h2 = e.host_images()
     h1[:] = f1
@@ -213,23 +187,23 @@ def run_ours(args, rank, world, local):
             ends[k].record(ext)
         e.synchronize()
         torch.cuda.synchronize()
-        dist_barrier(world)
+        R.barrier(world)
         ms = [starts[k].elapsed_time(ends[k]) for k in range(args.steps)]
 
         # end to end through the C-ABI with host buffers (pinned frames in, field out)
         e.set_device_images(0, 0)
         e.run_pair()
         e.field(3)
-        dist_barrier(world)
+        R.barrier(world)
         t0 = time.perf_counter()
         for _ in range(args.steps):
             e.run_pair()
             _, _, dx, dy, vv = e.field(3)
         e2e_local = time.perf_counter() - t0
-    total_s = dist_max(sum(ms) / 1e3, world)
-    value = world * args.steps * nvec / total_s
-    e2e_s = dist_max(e2e_local, world)
-    e2e = {"value": world * args.steps * nvec / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 2 * NX * NY,
+    total_s = R.max_over_ranks(sum(ms) / 1e3, world)
+    value = R.throughput(args.steps * nvec, sum(ms) / 1e3, world)
+    e2e_s = R.max_over_ranks(e2e_local, world)
+    e2e = {"value": R.sum_over_ranks(args.steps * nvec, world) / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 2 * NX * NY,
            "d2h_bytes_per_step": int(dx.nbytes + dy.nbytes + vv.nbytes)}
 
     # live roofline of the dominant kernel (grid-2 correlation), on the engine stream
@@ -320,13 +294,10 @@ def main():
         if out is not None:
             print(json.dumps(out))
         return
-    rank, world, local = dist_setup(args.gpus)
+    R = replicas()
+    rank, world, local = R.init("nccl")
     out = run_ours(args, rank, world, local)
-    if world > 1:
-        import torch.distributed as dist
-
-        dist.barrier()
-        dist.destroy_process_group()
+    R.finish(world)
     if rank == 0 and out is not None:
         print(json.dumps(out))
 

@@ -187,6 +187,10 @@ int piv_write_tecplot(piv_engine *e, const char *path, int selection);
 int piv_tecplot_write_arrays(const char *path, int Nx_vec, int Ny_vec, int spacing_x, int spacing_y, int raw,
                              int Npeak_save, const float *dx, const float *dy);
 
+/* Binary sidecar (no counterpart in the reference): a float32 array of `ndim` dimensions
+ * as a NumPy .npy file (format 1.0, little-endian, C order). */
+int piv_npy_write_f32(const char *path, const float *data, int ndim, const int *shape);
+
 /* Baseline TIFF (CImageIO, X/ImageIOPkg.cpp:124-428 and :641): uncompressed, 8-bit grey,
  * strip-organised, either byte order.  piv_tiff_read8 needs the file to be exactly Nx x Ny
  * (PIV_ERR_ARG otherwise, PIV_ERR_UNSUPPORTED for other bit depths or compression). */

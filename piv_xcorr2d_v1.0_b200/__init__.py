@@ -120,6 +120,7 @@ EXPORTS = {
     "piv_write_tecplot": (C.c_int, [_P, C.c_char_p, C.c_int]),
     "piv_tecplot_write_arrays": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _F, _F]),
     "piv_output_name": (C.c_int, [C.POINTER(PivParams), C.c_char_p, C.c_int, C.c_int, C.c_char_p, C.c_size_t]),
+    "piv_npy_write_f32": (C.c_int, [C.c_char_p, _F, C.c_int, C.POINTER(C.c_int)]),
     "piv_tiff_info": (C.c_int, [C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "piv_tiff_read8": (C.c_int, [C.c_char_p, _U8, C.c_int, C.c_int]),
     "piv_tiff_write8": (C.c_int, [C.c_char_p, _U8, C.c_int, C.c_int]),

@@ -221,6 +221,33 @@ int piv_tecplot_write_arrays(const char *path, int Nx_vec, int Ny_vec, int sp_x,
     return (ok && closed) ? PIV_OK : PIV_ERR_IO;
 }
 
+// ---- binary sidecar: NPY v1.0, little-endian float32, C order ----
+int piv_npy_write_f32(const char *path, const float *data, int ndim, const int *shape)
+{
+    if (!path || !data || !shape || ndim < 1 || ndim > 8) return PIV_ERR_ARG;
+    size_t n = 1;
+    std::string sh = "(";
+    for (int d = 0; d < ndim; ++d) {
+        if (shape[d] < 0) return PIV_ERR_ARG;
+        n *= (size_t)shape[d];
+        sh += std::to_string(shape[d]) + (ndim == 1 ? "," : (d + 1 < ndim ? ", " : ""));
+    }
+    sh += ")";
+    std::string hdr = "{'descr': '<f4', 'fortran_order': False, 'shape': " + sh + ", }";
+    const size_t pre = 10;  // magic(6) + version(2) + header length(2)
+    size_t total = pre + hdr.size() + 1;
+    hdr.append((64 - total % 64) % 64, ' ');
+    hdr.push_back('\n');
+    FILE *f = fopen(path, "wb");
+    if (!f) return PIV_ERR_IO;
+    const unsigned char magic[8] = {0x93, 'N', 'U', 'M', 'P', 'Y', 1, 0};
+    const uint16_t hl = (uint16_t)hdr.size();
+    const unsigned char hlb[2] = {(unsigned char)(hl & 0xff), (unsigned char)(hl >> 8)};
+    bool ok = fwrite(magic, 1, 8, f) == 8 && fwrite(hlb, 1, 2, f) == 2 &&
+              fwrite(hdr.data(), 1, hdr.size(), f) == hdr.size() && fwrite(data, sizeof(float), n, f) == n;
+    return (fclose(f) == 0 && ok) ? PIV_OK : PIV_ERR_IO;
+}
+
 // ---- minimal baseline TIFF (uncompressed, 8-bit grey, strips; both byte orders) ----
 
 namespace {

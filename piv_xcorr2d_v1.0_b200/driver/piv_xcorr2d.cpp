@@ -1,7 +1,7 @@
 // piv_xcorr2d -- command-line driver, a Linux replacement for X/main.cpp of
 // xinzhixue/PIV_xcorr2d_V1.0 (X/ = xcorr2d_V1.0/) on top of the C-ABI.
 //
-//   piv_xcorr2d [Parameter.dat] [--overlap]
+//   piv_xcorr2d [Parameter.dat] [--overlap] [--resume] [--npy] [--shard r/W]
 //
 // Reads the 50-line parameter file (default ./Parameter.dat), the image-pair index list,
 // and for every index NNNN the frames prefix1+NNNN+suffix1 and prefix2+NNNN+suffix2
@@ -12,6 +12,11 @@
 //
 // --overlap: reads the next pair's frames and writes the previous pair's files on host
 // threads while the GPU processes the current pair.
+// --resume:  skips pairs whose output files all exist already.
+// --npy:     also writes every field as a float32 .npy sidecar next to its .dat file
+//            ([Ny_vec][Nx_vec][2] filtered, [Ny_vec][Nx_vec][Npeak_save][2] raw).
+// --shard r/W: processes pairs r, r+W, r+2W, ... of the list (replicas: run W processes,
+//            one per GPU, e.g. with CUDA_VISIBLE_DEVICES=r; pairs are independent).
 #include <sys/stat.h>
 #include <sys/types.h>
 
@@ -84,7 +89,17 @@ int fetch(piv_engine *e, const piv_params &p, const piv_geometry &g, PairOutput 
     return rc;
 }
 
-int write_outputs(const piv_params &p, const piv_geometry &g, const char *folder, const PairOutput &o)
+int n_kinds(const piv_params &p) { return p.Npass2 > 0 ? 5 : 2; }
+
+bool outputs_exist(const piv_params &p, const char *folder, int idx)
+{
+    char path[4096];
+    for (int kind = 0; kind < n_kinds(p); ++kind)
+        if (piv_output_name(&p, folder, idx, kind, path, sizeof(path)) || !file_exists(path)) return false;
+    return true;
+}
+
+int write_outputs(const piv_params &p, const piv_geometry &g, const char *folder, const PairOutput &o, bool npy)
 {
     char path[4096];
     int rc = 0;
@@ -94,6 +109,19 @@ int write_outputs(const piv_params &p, const piv_geometry &g, const char *folder
         const int spx = grid ? p.spacing_x2 : p.spacing_x1, spy = grid ? p.spacing_y2 : p.spacing_y1;
         rc = piv_tecplot_write_arrays(path, g.Nx_vec[grid], g.Ny_vec[grid], spx, spy, raw ? 1 : 0, p.Npeak_save,
                                       x.data(), y.data());
+        if (rc || !npy) return;
+        std::string np(path);
+        if (np.size() > 4 && np.compare(np.size() - 4, 4, ".dat") == 0) np.resize(np.size() - 4);
+        np += ".npy";
+        std::vector<float> xy(x.size() * 2);
+        for (size_t i = 0; i < x.size(); ++i) {
+            xy[2 * i] = x[i];
+            xy[2 * i + 1] = y[i];
+        }
+        const int shape_raw[4] = {g.Ny_vec[grid], g.Nx_vec[grid], p.Npeak_save, 2};
+        const int shape_f[3] = {g.Ny_vec[grid], g.Nx_vec[grid], 2};
+        rc = raw ? piv_npy_write_f32(np.c_str(), xy.data(), 4, shape_raw)
+                 : piv_npy_write_f32(np.c_str(), xy.data(), 3, shape_f);
     };
     w(0, 0, true, o.raw1x, o.raw1y);
     w(1, 0, false, o.f1x, o.f1y);
@@ -111,10 +139,19 @@ int write_outputs(const piv_params &p, const piv_geometry &g, const char *folder
 int main(int argc, char **argv)
 {
     const char *param_path = "Parameter.dat";
-    bool overlap = false;
+    bool overlap = false, resume = false, npy = false;
+    int shard_r = 0, shard_w = 1;
     for (int i = 1; i < argc; ++i) {
         if (!strcmp(argv[i], "--overlap")) overlap = true;
-        else param_path = argv[i];
+        else if (!strcmp(argv[i], "--resume")) resume = true;
+        else if (!strcmp(argv[i], "--npy")) npy = true;
+        else if (!strcmp(argv[i], "--shard") && i + 1 < argc) {
+            if (sscanf(argv[++i], "%d/%d", &shard_r, &shard_w) != 2 || shard_w < 1 || shard_r < 0 ||
+                shard_r >= shard_w) {
+                printf("--shard expects r/W with 0 <= r < W\n");
+                return 1;
+            }
+        } else param_path = argv[i];
     }
     piv_params p;
     piv_paths paths;
@@ -141,6 +178,26 @@ int main(int argc, char **argv)
     if (pairs.empty()) {
         printf("No image pair index detected!\n");
         return 1;
+    }
+    if (shard_w > 1) {
+        std::vector<int> mine;
+        for (size_t i = (size_t)shard_r; i < pairs.size(); i += (size_t)shard_w) mine.push_back(pairs[i]);
+        pairs.swap(mine);
+    }
+    if (resume) {
+        std::vector<int> todo;
+        for (int idx : pairs)
+            if (!outputs_exist(p, paths.folder_result, idx)) todo.push_back(idx);
+        printf("Resuming: %zu of %zu pairs have outputs already\n", pairs.size() - todo.size(), pairs.size());
+        pairs.swap(todo);
+        if (pairs.empty()) {
+            printf("NO ERROR!\n");
+            return 0;
+        }
+    }
+    if (pairs.empty()) {
+        printf("NO ERROR!\n");
+        return 0;
     }
     if (!make_dirs(paths.folder_result)) {
         printf("Folder creation not successful!\n");
@@ -217,8 +274,8 @@ int main(int argc, char **argv)
         }
         if (overlap) {
             pending = std::move(out);
-            writer = std::thread([&] { writer_rc = write_outputs(p, g, paths.folder_result, pending); });
-        } else if (write_outputs(p, g, paths.folder_result, out)) {
+            writer = std::thread([&] { writer_rc = write_outputs(p, g, paths.folder_result, pending, npy); });
+        } else if (write_outputs(p, g, paths.folder_result, out, npy)) {
             status = false;
             break;
         }

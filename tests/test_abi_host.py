@@ -223,6 +223,18 @@ def test_tiff_roundtrip_and_big_endian(tmp_path):
     assert np.array_equal(out, img)
 
 
+@pytest.mark.parametrize("shape", [(7,), (3, 5), (2, 3, 4), (11, 13, 4, 2)])
+def test_npy_sidecar_roundtrip(tmp_path, shape):
+    import ctypes as C
+
+    a = np.random.default_rng(0).normal(size=shape).astype(np.float32)
+    f = tmp_path / "a.npy"
+    dims = (C.c_int * len(shape))(*shape)
+    assert P.lib().piv_npy_write_f32(str(f).encode(), a.ctypes.data_as(P._F), len(shape), dims) == 0
+    b = np.load(f)
+    assert b.dtype == np.float32 and b.shape == shape and np.array_equal(a, b)
+
+
 def test_synth_pair_deterministic_and_seeded():
     s = P.synth_params(96, 64, ppp=0.05, field=P.PIV_FIELD_UNIFORM, a=3.3, b=-1.7, seed=9)
     a1, a2 = P.synth_pair(s)

@@ -61,6 +61,40 @@ def test_driver_end_to_end(cuda, tmp_path, overlap):
     assert abs(np.median(dx) - 2.8) < 0.1
 
 
+def test_driver_shards_resume_and_npy(cuda, tmp_path):
+    pairs = [2, 3, 5, 8, 13]
+    par = write_setup(tmp_path, pairs)
+    p, paths = P.read_params(par)
+    # two replicas (one GPU here, run one after the other): each takes every other pair
+    for r in range(2):
+        out = subprocess.run([str(EXE), str(par), "--shard", f"{r}/2", "--npy"], capture_output=True, text=True,
+                             timeout=300)
+        assert out.returncode == 0, out.stdout + out.stderr
+        assert out.stdout.count("Done!") == len(pairs[r::2])
+    for idx in pairs:
+        for kind in range(5):
+            dat = Path(P.output_name(p, paths["folder_result"], idx, kind))
+            assert dat.exists()
+            arr = np.load(dat.with_suffix(".npy"))
+            lines = dat.read_text().splitlines()[3:]
+            if kind in (0, 2):
+                assert arr.shape[2:] == (p.Npeak_save, 2)
+                first = np.array([[float(v) for v in l.split("\t")[2:4]] for l in lines])
+                assert np.allclose(arr[:, :, 0, :].reshape(-1, 2), first, atol=0.0051)
+            else:
+                assert arr.shape[2] == 2
+                vals = np.array([[float(v) for v in l.split("\t")[2:4]] for l in lines])
+                assert np.allclose(arr.reshape(-1, 2), vals, atol=0.0051)
+    # everything is there: --resume does nothing
+    out = subprocess.run([str(EXE), str(par), "--resume"], capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0 and "Resuming: 5 of 5" in out.stdout and "Done!" not in out.stdout
+    # one output removed: only that pair runs again
+    Path(P.output_name(p, paths["folder_result"], 8, 4)).unlink()
+    out = subprocess.run([str(EXE), str(par), "--resume"], capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0 and "Resuming: 4 of 5" in out.stdout and out.stdout.count("Done!") == 1
+    assert Path(P.output_name(p, paths["folder_result"], 8, 4)).exists()
+
+
 def test_driver_error_paths(cuda, tmp_path):
     r = subprocess.run([str(EXE), str(tmp_path / "nope.dat")], capture_output=True, text=True, timeout=60)
     assert r.returncode == 1 and "Can't open parameter file!" in r.stdout
