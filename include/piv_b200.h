@@ -242,6 +242,19 @@ int piv_get_stream(const piv_engine *e, void **stream);
  * the tuning input (0 if not tuned; PIV_AUTOTUNE=0 keeps the defaults). */
 int piv_xcorr_config(const piv_engine *e, int grid, int *windows_per_cta, int *threads_per_cta, float *tuned_ms);
 
+/* Correlation path of a grid.  PIV_XCORR_SIMT: register FFTs in FP32 on the CUDA cores
+ * (default).  PIV_XCORR_TC_SPLIT: the transforms as DFT products on the tcgen05 tensor
+ * cores with split-BF16 operands (hi*hi + hi*lo + lo*hi, FP32 accumulation).
+ * PIV_XCORR_TC_BF16: one BF16 product per step (precision study only).  The tensor-core
+ * paths cover square 16x16, 32x32 and 64x64 windows (PIV_ERR_UNSUPPORTED otherwise).
+ * PIV_XCORR_PATH=tc|tc1 in the environment at piv_create selects them for every grid
+ * they cover. */
+#define PIV_XCORR_SIMT 0
+#define PIV_XCORR_TC_SPLIT 1
+#define PIV_XCORR_TC_BF16 2
+int piv_set_xcorr_path(piv_engine *e, int grid, int path);
+int piv_get_xcorr_path(const piv_engine *e, int grid, int *path);
+
 /* Kernels that one piv_run_pair launches with the engine's parameters. */
 int piv_kernel_launches_per_pair(const piv_engine *e, int *n);
 
@@ -255,6 +268,14 @@ int piv_time_stage(piv_engine *e, int which, int reps, float *ms_per_launch);
 /* Measured FP32 FMA throughput of the current device (TFLOP/s, 2 flops per FMA), from a
  * dependent-chain FMA kernel over every SM; the SIMT roofline of the FP32 correlation path. */
 int piv_probe_fp32_peak(float *tflops);
+
+/* Tensor-core self-check: D[128][N] = A[128][K] * B[N][K]^T computed by tcgen05 MMAs
+ * with BF16 operands staged in shared memory (a_mn / b_mn: operand in the MN-major
+ * instead of the K-major layout) and FP32 accumulation in tensor memory; nprod 1 uses
+ * the rounded operands, 3 the split hi*hi + hi*lo + lo*hi.  Host arrays, row-major.
+ * N and K: multiples of 16 in [16, 128].  PIV_ERR_UNSUPPORTED on a device other than
+ * compute capability 10.x. */
+int piv_tc_gemm_check(const float *A, const float *B, float *D, int N, int K, int a_mn, int b_mn, int nprod);
 
 /* ---- standalone MHE (mhe_gpu) --------------------------------------------- */
 

@@ -34,6 +34,10 @@ PIV_ERR_IO = -6
 PIV_ERR_STATE = -7
 PIV_ERR_DEVICE = -8
 
+PIV_XCORR_SIMT = 0
+PIV_XCORR_TC_SPLIT = 1
+PIV_XCORR_TC_BF16 = 2
+
 PIV_FIELD_UNIFORM = 0
 PIV_FIELD_VORTEX = 1
 PIV_FIELD_FOURIER = 2
@@ -136,6 +140,9 @@ EXPORTS = {
     "piv_kernel_launches_per_pair": (C.c_int, [_P, C.POINTER(C.c_int)]),
     "piv_time_stage": (C.c_int, [_P, C.c_int, C.c_int, _F]),
     "piv_probe_fp32_peak": (C.c_int, [_F]),
+    "piv_set_xcorr_path": (C.c_int, [_P, C.c_int, C.c_int]),
+    "piv_get_xcorr_path": (C.c_int, [_P, C.c_int, C.POINTER(C.c_int)]),
+    "piv_tc_gemm_check": (C.c_int, [_F, _F, _F, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]),
     "piv_mhe_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_float, C.POINTER(_P)]),
     "piv_mhe_process": (C.c_int, [_P, _P, _P, _P]),
     "piv_mhe_destroy": (C.c_int, [_P]),
@@ -431,6 +438,14 @@ class Engine:
         self._ck(lib().piv_time_stage(self.h, which, reps, C.byref(ms)))
         return ms.value
 
+    def set_xcorr_path(self, grid, path):
+        self._ck(lib().piv_set_xcorr_path(self.h, grid, path))
+
+    def xcorr_path(self, grid):
+        v = C.c_int(0)
+        self._ck(lib().piv_get_xcorr_path(self.h, grid, C.byref(v)))
+        return v.value
+
 
 def fp32_peak_tflops():
     t = C.c_float(0)
@@ -438,6 +453,19 @@ def fp32_peak_tflops():
     if rc != PIV_OK:
         raise PivError(rc, "FP32 peak probe failed")
     return t.value
+
+
+def tc_gemm_check(A, B, a_mn=False, b_mn=False, nprod=3):
+    """A (128 x K) times B (N x K) transposed on the tcgen05 tensor-core path."""
+    A = np.ascontiguousarray(A, np.float32)
+    B = np.ascontiguousarray(B, np.float32)
+    assert A.shape[0] == 128 and A.shape[1] == B.shape[1]
+    D = np.empty((128, B.shape[0]), np.float32)
+    rc = lib().piv_tc_gemm_check(_ptr(A, C.c_float), _ptr(B, C.c_float), _ptr(D, C.c_float), B.shape[0],
+                                 A.shape[1], int(a_mn), int(b_mn), nprod)
+    if rc != PIV_OK:
+        raise PivError(rc, "tensor-core check failed")
+    return D
 
 
 class xcorr2d_multi:

@@ -121,6 +121,7 @@ struct GridState {
     bool last_deformed = false;
     bool has_pass = false;
     int variant = 0;          // fused-kernel instantiation chosen by the autotuner
+    int path = PIV_XCORR_SIMT;  // correlation path (PIV_XCORR_*)
     float tuned_ms[8] = {};   // measured time per variant (0 = not measured)
     int n_tuned = 0;
 };
@@ -293,11 +294,16 @@ int do_xcorr(piv_engine *e, int k, bool deformed, int first, int end, float *dum
     a.pidx = gs.pidx;
     a.pval = gs.pval;
     a.cc_dump = dump;
+    a.status = e->d_status;
     const char *why = nullptr;
+    auto launch = [&]() {
+        if (gs.path == PIV_XCORR_SIMT) return launch_xcorr(a, deformed, e->stream, &why, gs.variant);
+        return launch_xcorr_tc(a, deformed, e->stream, &why, gs.path == PIV_XCORR_TC_SPLIT ? 3 : 1);
+    };
     if (dump) {
         a.w_first = first;
         a.w_end = end;
-        cudaError_t c = launch_xcorr(a, deformed, e->stream, &why, gs.variant);
+        cudaError_t c = launch();
         if (c != cudaSuccess) return set_err(e, PIV_ERR_CUDA, "correlation kernel: %s", why ? why : cudaGetErrorString(c));
         return PIV_OK;
     }
@@ -306,7 +312,7 @@ int do_xcorr(piv_engine *e, int k, bool deformed, int first, int end, float *dum
     for (int i = 0; i < Nsec; ++i) {
         a.w_first = i * Neach;
         a.w_end = a.w_first + (i == Nsec - 1 ? Nlast : Neach);
-        cudaError_t c = launch_xcorr(a, deformed, e->stream, &why, gs.variant);
+        cudaError_t c = launch();
         if (c != cudaSuccess) return set_err(e, PIV_ERR_CUDA, "correlation kernel: %s", why ? why : cudaGetErrorString(c));
     }
     return PIV_OK;
@@ -665,6 +671,13 @@ int piv_create(const piv_params *p, piv_engine **out)
         }
     }
     if ((rc = tune_xcorr(e))) return bail(rc);
+    if (const char *path = getenv("PIV_XCORR_PATH")) {
+        // "tc": split-BF16 tensor-core path, "tc1": single-product BF16 (precision study),
+        // for every grid whose window shape the tensor-core path covers
+        const int want = !strcmp(path, "tc") ? PIV_XCORR_TC_SPLIT : !strcmp(path, "tc1") ? PIV_XCORR_TC_BF16 : PIV_XCORR_SIMT;
+        for (int k = 0; k < 2; ++k)
+            if (xcorr_tc_supported(e->grid[k].gg.ws_x, e->grid[k].gg.ws_y)) e->grid[k].path = want;
+    }
     if (getenv("PIV_TIMING") && atoi(getenv("PIV_TIMING")) == 1) {
         e->timing = true;
         for (auto &ev : e->ev) cudaEventCreate(&ev);
@@ -845,7 +858,9 @@ int piv_synchronize(piv_engine *e)
         const int st = *e->h_status;
         CK(cudaMemsetAsync(e->d_status, 0, sizeof(int), e->stream));
         CK(cudaStreamSynchronize(e->stream));
-        return set_err(e, PIV_ERR_DEVICE, "device status 0x%x (hole-fill iteration cap reached)", st);
+        return set_err(e, PIV_ERR_DEVICE, "device status 0x%x (%s)", st,
+                       (st & kStatusMmaWait) ? "tensor-core MMA completion wait timed out"
+                                             : "hole-fill iteration cap reached");
     }
     if (e->timing && e->have_times) {
         cudaEventElapsedTime(&e->stage_ms[0], e->ev[0], e->ev[1]);
@@ -981,6 +996,28 @@ int piv_debug_cc_planes(piv_engine *e, int grid, int first, int n, float *out)
 }
 
 // ---- measurement -----------------------------------------------------------------
+
+int piv_set_xcorr_path(piv_engine *e, int grid, int path)
+{
+    if (!e || (grid != 1 && grid != 2) || path < PIV_XCORR_SIMT || path > PIV_XCORR_TC_BF16) return PIV_ERR_ARG;
+    GridState &gs = e->grid[grid - 1];
+    if (path != PIV_XCORR_SIMT && !xcorr_tc_supported(gs.gg.ws_x, gs.gg.ws_y))
+        return set_err(e, PIV_ERR_UNSUPPORTED, "window shape %dx%d has no tensor-core path", gs.gg.ws_x, gs.gg.ws_y);
+    if (gs.path != path && e->graph) {
+        cudaStreamSynchronize(e->stream);
+        cudaGraphExecDestroy(e->graph);
+        e->graph = nullptr;
+    }
+    gs.path = path;
+    return PIV_OK;
+}
+
+int piv_get_xcorr_path(const piv_engine *e, int grid, int *path)
+{
+    if (!e || (grid != 1 && grid != 2) || !path) return PIV_ERR_ARG;
+    *path = e->grid[grid - 1].path;
+    return PIV_OK;
+}
 
 int piv_xcorr_config(const piv_engine *e, int grid, int *windows_per_cta, int *threads_per_cta, float *tuned_ms)
 {

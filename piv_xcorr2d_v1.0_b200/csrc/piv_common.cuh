@@ -125,6 +125,7 @@ struct XcorrArgs {
     int32_t *pidx;             // [Nt_vec][Nps]
     float *pval;               // [Nt_vec][Nps]
     float *cc_dump;            // optional [n][ws_y][ws_x], window w -> cc_dump + (w - w_first)*ws_x*ws_y
+    int *status;               // device status word (tensor-core path: kStatusMmaWait), may be null
 };
 
 // Launches the fused correlation + peak kernel for the window range of a.
@@ -134,6 +135,9 @@ cudaError_t launch_xcorr(const XcorrArgs &a, bool deformed, cudaStream_t s, cons
 bool xcorr_supported(int ws_x, int ws_y);
 int xcorr_variants(int ws_x, int ws_y);
 bool xcorr_variant_shape(int ws_x, int ws_y, int variant, int *windows_per_cta, int *threads_per_cta);
+// Tensor-core path (xcorr_tc.cuh): nprod 3 = split-BF16 (hi*hi + hi*lo + lo*hi), 1 = BF16.
+bool xcorr_tc_supported(int ws_x, int ws_y);
+cudaError_t launch_xcorr_tc(const XcorrArgs &a, bool deformed, cudaStream_t s, const char **why, int nprod);
 
 // Field kernels (field_kernels.cu).
 struct DeformArgs {
@@ -187,6 +191,6 @@ cudaError_t launch_mhe(const MheGeom &m, const uint8_t *in, int in_pitch, int *l
                        int ox, int oy, cudaStream_t s);
 
 // Status bits written by kernels.
-enum : int { kStatusFillCap = 1 };
+enum : int { kStatusFillCap = 1, kStatusMmaWait = 2 };
 
 }  // namespace piv

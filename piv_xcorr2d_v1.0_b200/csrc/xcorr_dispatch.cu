@@ -120,3 +120,34 @@ cudaError_t launch_xcorr(const XcorrArgs &a, bool deformed, cudaStream_t s, cons
 }
 
 }  // namespace piv
+
+namespace piv {
+
+template <int WS, int NPROD>
+cudaError_t launch_tc_shape(const XcorrArgs &a, bool deformed, int K, cudaStream_t s);
+extern template cudaError_t launch_tc_shape<16, 3>(const XcorrArgs &, bool, int, cudaStream_t);
+extern template cudaError_t launch_tc_shape<16, 1>(const XcorrArgs &, bool, int, cudaStream_t);
+extern template cudaError_t launch_tc_shape<32, 3>(const XcorrArgs &, bool, int, cudaStream_t);
+extern template cudaError_t launch_tc_shape<32, 1>(const XcorrArgs &, bool, int, cudaStream_t);
+extern template cudaError_t launch_tc_shape<64, 3>(const XcorrArgs &, bool, int, cudaStream_t);
+extern template cudaError_t launch_tc_shape<64, 1>(const XcorrArgs &, bool, int, cudaStream_t);
+
+bool xcorr_tc_supported(int wsx, int wsy) { return wsx == wsy && (wsx == 16 || wsx == 32 || wsx == 64); }
+
+cudaError_t launch_xcorr_tc(const XcorrArgs &a, bool deformed, cudaStream_t s, const char **why, int nprod)
+{
+    if (a.g.Nps > 8) {
+        if (why) *why = "Npeak_save > 8 is not built into this engine";
+        return cudaErrorInvalidValue;
+    }
+    if (!xcorr_tc_supported(a.g.ws_x, a.g.ws_y) || (nprod != 1 && nprod != 3)) {
+        if (why) *why = "window shape not built into the tensor-core path";
+        return cudaErrorInvalidValue;
+    }
+    const int K = a.g.Nps <= 4 ? 4 : 8;
+    if (a.g.ws_x == 16) return nprod == 3 ? launch_tc_shape<16, 3>(a, deformed, K, s) : launch_tc_shape<16, 1>(a, deformed, K, s);
+    if (a.g.ws_x == 32) return nprod == 3 ? launch_tc_shape<32, 3>(a, deformed, K, s) : launch_tc_shape<32, 1>(a, deformed, K, s);
+    return nprod == 3 ? launch_tc_shape<64, 3>(a, deformed, K, s) : launch_tc_shape<64, 1>(a, deformed, K, s);
+}
+
+}  // namespace piv

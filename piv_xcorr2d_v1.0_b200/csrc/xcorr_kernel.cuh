@@ -123,6 +123,125 @@ __device__ __forceinline__ void topk_insert(float (&tv)[K], int (&ti)[K], float 
     }
 }
 
+// ------------------------------------------------------------------------------
+// Peak stage of one window (one warp): 4-neighbour local maxima inside the search
+// region, count, top-Npeak_save, 3-point Gaussian fit, predictor, limits, NaN/Inf
+// removal (find_local_max_2d, reduce_max_index_*, replace_local_max_2d,
+// peak_subpixel_4peak_2d, kernel_remove_nan).  P: the window's fftshifted plane in
+// shared memory with row stride WSX + 1.
+// ------------------------------------------------------------------------------
+template <int WSX, int WSY, int K>
+__device__ __forceinline__ void peak_window(const XcorrArgs &a, const float *P, int w, int lane)
+{
+    constexpr int LDF = WSX + 1;
+    const GridGeom &g = a.g;
+    const int rows = WSY - 2 * g.by;
+    if (a.cc_dump) {
+        // diagnostic mode: planes only, the pass outputs stay untouched
+        float *dst = a.cc_dump + (size_t)(w - a.w_first) * (WSX * WSY);
+        for (int t = lane; t < WSX * WSY; t += 32) {
+            const int j = t / WSX, i = t - j * WSX;
+            dst[t] = P[j * LDF + i];
+        }
+        return;
+    }
+    // lane-local top-K of the lane's region rows, sorted (value desc, index asc)
+    float tv[K];
+    int ti[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        tv[k] = -1.f;
+        ti[k] = INT_MAX;
+    }
+    int cnt = 0;
+    for (int jj = lane; jj < rows; jj += 32) {
+        const int j = g.by + jj;
+        const float *pm = P + j * LDF;
+        float mid[WSX];
+#pragma unroll
+        for (int i = 0; i < WSX; ++i) mid[i] = pm[i];
+#pragma unroll
+        for (int i = 1; i < WSX - 1; ++i) {
+            const float v = mid[i];
+            // branch-free local-maximum test (bitwise &, no short circuit)
+            const bool c = (i >= g.bx) & (i <= WSX - 1 - g.bx) & (v > 0.f) & (v >= mid[i - 1]) &
+                           (v >= mid[i + 1]) & (v >= pm[i - LDF]) & (v >= pm[i + LDF]);
+            cnt += c;
+            if (c && better(v, j * WSX + i, tv[K - 1], ti[K - 1])) topk_insert<K>(tv, ti, v, j * WSX + i);
+        }
+    }
+#pragma unroll
+    for (int off = 16; off >= 1; off >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, off);
+    // the window's top Nps: Nps rounds of a warp arg-max over the lanes' list heads;
+    // indices are unique, so exactly one lane owns each winner and pops it
+    float v = -1.f;
+    int idx = INT_MAX;
+    for (int k = 0; k < g.Nps; ++k) {
+        float bv = tv[0];
+        int bi = ti[0];
+#pragma unroll
+        for (int off = 16; off >= 1; off >>= 1) {
+            const float ov = __shfl_xor_sync(0xffffffffu, bv, off);
+            const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
+            if (better(ov, oi, bv, bi)) {
+                bv = ov;
+                bi = oi;
+            }
+        }
+        if (lane == k) {
+            v = bv;
+            idx = bi;
+        }
+        if (bi == ti[0] && bv > 0.f) {
+#pragma unroll
+            for (int s = 0; s < K - 1; ++s) {
+                tv[s] = tv[s + 1];
+                ti[s] = ti[s + 1];
+            }
+            tv[K - 1] = -1.f;
+            ti[K - 1] = INT_MAX;
+        }
+    }
+    if (lane < g.Nps) {
+        float ox = 0.f, oy = 0.f;
+        bool ok = false;
+        if (v > 0.f) {
+            const int j = idx / WSX, i = idx - j * WSX;
+            if (i != 0 && i != WSX - 1 && j != 0 && j != WSY - 1) {
+                const float *pc = P + j * LDF + i;
+                const float c0 = pc[-1], c2 = pc[1], d0 = pc[-LDF], d2 = pc[LDF];
+                const double dv = (double)v * (double)v;
+                // numerator ln f- - ln f+ in FP32 as the reference; the cancelling
+                // denominator ln(f- f+ / f0^2) in FP64
+                const float nx = logf(c0) - logf(c2), ny = logf(d0) - logf(d2);
+                const double denx = log(((double)c0 * (double)c2) / dv);
+                const double deny = log(((double)d0 * (double)d2) / dv);
+                const float sx = (float)((double)nx / denx / 2.0), sy = (float)((double)ny / deny / 2.0);
+                ox = (float)i + sx - (float)WSX / 2 + a.pred_x[w];
+                oy = (float)j + sy - (float)WSY / 2 + a.pred_y[w];
+                ok = true;
+                if (ox < g.lx1 || ox > g.lx2 || oy < g.ly1 || oy > g.ly2) {
+                    ok = false;
+                    ox = 0.f;
+                    oy = 0.f;
+                }
+                if (isnan(ox) || isnan(oy) || isinf(ox) || isinf(oy)) {
+                    ok = false;
+                    ox = 0.f;
+                    oy = 0.f;
+                }
+            }
+        }
+        const size_t o = (size_t)w * g.Nps + lane;
+        a.cdx[o] = ox;
+        a.cdy[o] = oy;
+        a.cvalid[o] = ok ? 1 : 0;
+        a.pidx[o] = (v > 0.f) ? idx : -1;
+        a.pval[o] = (v > 0.f) ? v : 0.f;
+    }
+    if (lane == 0) a.count[w] = cnt;
+}
+
 template <int WSX, int WSY, int B, int NT, int K, bool DEF>
 __global__ void __launch_bounds__(NT) xcorr_peak_kernel(const XcorrArgs a)
 {
@@ -236,115 +355,11 @@ __global__ void __launch_bounds__(NT) xcorr_peak_kernel(const XcorrArgs a)
     // ---------------- P5: peaks, warp per window ----------------
     const int warp = tid >> 5, lane = tid & 31;
     constexpr int NW = NT / 32;
-    const int rows = WSY - 2 * g.by;
     for (int b = warp; b < B; b += NW) {
         const int w = w_base + b;
         if (w >= a.w_end) continue;
         const float *P = reinterpret_cast<const float *>(sm + ((b & ~1) + 1) * WIN) + (b & 1) * (WSY * LDF);
-        if (a.cc_dump) {
-            // diagnostic mode: planes only, the pass outputs stay untouched
-            float *dst = a.cc_dump + (size_t)(w - a.w_first) * (WSX * WSY);
-            for (int t = lane; t < WSX * WSY; t += 32) {
-                const int j = t / WSX, i = t - j * WSX;
-                dst[t] = P[j * LDF + i];
-            }
-            continue;
-        }
-        // lane-local top-K of the lane's region rows, sorted (value desc, index asc)
-        float tv[K];
-        int ti[K];
-#pragma unroll
-        for (int k = 0; k < K; ++k) {
-            tv[k] = -1.f;
-            ti[k] = INT_MAX;
-        }
-        int cnt = 0;
-        for (int jj = lane; jj < rows; jj += 32) {
-            const int j = g.by + jj;
-            const float *pm = P + j * LDF;
-            float mid[WSX];
-#pragma unroll
-            for (int i = 0; i < WSX; ++i) mid[i] = pm[i];
-#pragma unroll
-            for (int i = 1; i < WSX - 1; ++i) {
-                const float v = mid[i];
-                // branch-free local-maximum test (bitwise &, no short circuit)
-                const bool c = (i >= g.bx) & (i <= WSX - 1 - g.bx) & (v > 0.f) & (v >= mid[i - 1]) &
-                               (v >= mid[i + 1]) & (v >= pm[i - LDF]) & (v >= pm[i + LDF]);
-                cnt += c;
-                if (c && better(v, j * WSX + i, tv[K - 1], ti[K - 1])) topk_insert<K>(tv, ti, v, j * WSX + i);
-            }
-        }
-#pragma unroll
-        for (int off = 16; off >= 1; off >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, off);
-        // the window's top Nps: Nps rounds of a warp arg-max over the lanes' list heads;
-        // indices are unique, so exactly one lane owns each winner and pops it
-        float v = -1.f;
-        int idx = INT_MAX;
-        for (int k = 0; k < g.Nps; ++k) {
-            float bv = tv[0];
-            int bi = ti[0];
-#pragma unroll
-            for (int off = 16; off >= 1; off >>= 1) {
-                const float ov = __shfl_xor_sync(0xffffffffu, bv, off);
-                const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
-                if (better(ov, oi, bv, bi)) {
-                    bv = ov;
-                    bi = oi;
-                }
-            }
-            if (lane == k) {
-                v = bv;
-                idx = bi;
-            }
-            if (bi == ti[0] && bv > 0.f) {
-#pragma unroll
-                for (int s = 0; s < K - 1; ++s) {
-                    tv[s] = tv[s + 1];
-                    ti[s] = ti[s + 1];
-                }
-                tv[K - 1] = -1.f;
-                ti[K - 1] = INT_MAX;
-            }
-        }
-        if (lane < g.Nps) {
-            float ox = 0.f, oy = 0.f;
-            bool ok = false;
-            if (v > 0.f) {
-                const int j = idx / WSX, i = idx - j * WSX;
-                if (i != 0 && i != WSX - 1 && j != 0 && j != WSY - 1) {
-                    const float *pc = P + j * LDF + i;
-                    const float c0 = pc[-1], c2 = pc[1], d0 = pc[-LDF], d2 = pc[LDF];
-                    const double dv = (double)v * (double)v;
-                    // numerator ln f- - ln f+ in FP32 as the reference; the cancelling
-                    // denominator ln(f- f+ / f0^2) in FP64
-                    const float nx = logf(c0) - logf(c2), ny = logf(d0) - logf(d2);
-                    const double denx = log(((double)c0 * (double)c2) / dv);
-                    const double deny = log(((double)d0 * (double)d2) / dv);
-                    const float sx = (float)((double)nx / denx / 2.0), sy = (float)((double)ny / deny / 2.0);
-                    ox = (float)i + sx - (float)WSX / 2 + a.pred_x[w];
-                    oy = (float)j + sy - (float)WSY / 2 + a.pred_y[w];
-                    ok = true;
-                    if (ox < g.lx1 || ox > g.lx2 || oy < g.ly1 || oy > g.ly2) {
-                        ok = false;
-                        ox = 0.f;
-                        oy = 0.f;
-                    }
-                    if (isnan(ox) || isnan(oy) || isinf(ox) || isinf(oy)) {
-                        ok = false;
-                        ox = 0.f;
-                        oy = 0.f;
-                    }
-                }
-            }
-            const size_t o = (size_t)w * g.Nps + lane;
-            a.cdx[o] = ox;
-            a.cdy[o] = oy;
-            a.cvalid[o] = ok ? 1 : 0;
-            a.pidx[o] = (v > 0.f) ? idx : -1;
-            a.pval[o] = (v > 0.f) ? v : 0.f;
-        }
-        if (lane == 0) a.count[w] = cnt;
+        peak_window<WSX, WSY, K>(a, P, w, lane);
     }
 }
 
