@@ -153,6 +153,19 @@ __device__ __forceinline__ void peak_window(const XcorrArgs &a, const float *P, 
         tv[k] = -1.f;
         ti[k] = INT_MAX;
     }
+    // columns allowed by the border (and by the 4-neighbour stencil) as a bitmask
+    constexpr int NWRD = (WSX + 31) / 32;
+    uint32_t allow[NWRD];
+#pragma unroll
+    for (int q = 0; q < NWRD; ++q) {
+        uint32_t m = 0;
+#pragma unroll
+        for (int b = 0; b < 32; ++b) {
+            const int i = 32 * q + b;
+            m |= (uint32_t)((i >= 1) & (i <= WSX - 2) & (i >= g.bx) & (i <= WSX - 1 - g.bx)) << b;
+        }
+        allow[q] = m;
+    }
     int cnt = 0;
     for (int jj = lane; jj < rows; jj += 32) {
         const int j = g.by + jj;
@@ -160,14 +173,26 @@ __device__ __forceinline__ void peak_window(const XcorrArgs &a, const float *P, 
         float mid[WSX];
 #pragma unroll
         for (int i = 0; i < WSX; ++i) mid[i] = pm[i];
+        // local-maximum test of every column without branches, as a bitmask
+        uint32_t mk[NWRD];
+#pragma unroll
+        for (int q = 0; q < NWRD; ++q) mk[q] = 0;
 #pragma unroll
         for (int i = 1; i < WSX - 1; ++i) {
             const float v = mid[i];
-            // branch-free local-maximum test (bitwise &, no short circuit)
-            const bool c = (i >= g.bx) & (i <= WSX - 1 - g.bx) & (v > 0.f) & (v >= mid[i - 1]) &
-                           (v >= mid[i + 1]) & (v >= pm[i - LDF]) & (v >= pm[i + LDF]);
-            cnt += c;
-            if (c && better(v, j * WSX + i, tv[K - 1], ti[K - 1])) topk_insert<K>(tv, ti, v, j * WSX + i);
+            const bool c = (v > 0.f) & (v >= mid[i - 1]) & (v >= mid[i + 1]) & (v >= pm[i - LDF]) & (v >= pm[i + LDF]);
+            mk[i >> 5] |= (uint32_t)c << (i & 31);
+        }
+        // the row's maxima in column order into the lane's top-K
+#pragma unroll
+        for (int q = 0; q < NWRD; ++q) {
+            uint32_t m = mk[q] & allow[q];
+            cnt += __popc(m);
+            while (m) {
+                const int i = 32 * q + __ffs(m) - 1;
+                m &= m - 1;
+                topk_insert<K>(tv, ti, pm[i], j * WSX + i);
+            }
         }
     }
 #pragma unroll
