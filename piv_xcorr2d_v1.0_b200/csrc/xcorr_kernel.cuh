@@ -145,6 +145,12 @@ __device__ __forceinline__ void peak_window(const XcorrArgs &a, const float *P, 
         }
         return;
     }
+    // the predictor of the window, fetched early (used by the Nps fitting lanes)
+    float pred_x = 0.f, pred_y = 0.f;
+    if (lane < g.Nps) {
+        pred_x = a.pred_x[w];
+        pred_y = a.pred_y[w];
+    }
     // lane-local top-K of the lane's region rows, sorted (value desc, index asc)
     float tv[K];
     int ti[K];
@@ -197,22 +203,19 @@ __device__ __forceinline__ void peak_window(const XcorrArgs &a, const float *P, 
     }
 #pragma unroll
     for (int off = 16; off >= 1; off >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, off);
-    // the window's top Nps: Nps rounds of a warp arg-max over the lanes' list heads;
-    // indices are unique, so exactly one lane owns each winner and pops it
+    // the window's top Nps: Nps rounds of a warp arg-max over the lanes' list heads.
+    // Candidates are positive, so their bit patterns order as unsigned integers: the
+    // largest value is one warp max-reduction, the lowest index holding it one
+    // min-reduction (the order of better()).  Indices are unique, so exactly one lane
+    // owns each winner and pops it.
     float v = -1.f;
     int idx = INT_MAX;
     for (int k = 0; k < g.Nps; ++k) {
-        float bv = tv[0];
-        int bi = ti[0];
-#pragma unroll
-        for (int off = 16; off >= 1; off >>= 1) {
-            const float ov = __shfl_xor_sync(0xffffffffu, bv, off);
-            const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
-            if (better(ov, oi, bv, bi)) {
-                bv = ov;
-                bi = oi;
-            }
-        }
+        const uint32_t key = tv[0] > 0.f ? __float_as_uint(tv[0]) : 0u;
+        const uint32_t kmax = __reduce_max_sync(0xffffffffu, key);
+        const uint32_t imin = __reduce_min_sync(0xffffffffu, key == kmax ? (uint32_t)ti[0] : 0xffffffffu);
+        const float bv = kmax ? __uint_as_float(kmax) : -1.f;
+        const int bi = kmax ? (int)imin : INT_MAX;
         if (lane == k) {
             v = bv;
             idx = bi;
@@ -242,8 +245,8 @@ __device__ __forceinline__ void peak_window(const XcorrArgs &a, const float *P, 
                 const double denx = log(((double)c0 * (double)c2) / dv);
                 const double deny = log(((double)d0 * (double)d2) / dv);
                 const float sx = (float)((double)nx / denx / 2.0), sy = (float)((double)ny / deny / 2.0);
-                ox = (float)i + sx - (float)WSX / 2 + a.pred_x[w];
-                oy = (float)j + sy - (float)WSY / 2 + a.pred_y[w];
+                ox = (float)i + sx - (float)WSX / 2 + pred_x;
+                oy = (float)j + sy - (float)WSY / 2 + pred_y;
                 ok = true;
                 if (ox < g.lx1 || ox > g.lx2 || oy < g.ly1 || oy > g.ly2) {
                     ok = false;
