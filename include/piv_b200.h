@@ -242,7 +242,7 @@ int piv_get_stream(const piv_engine *e, void **stream);
  * the tuning input (0 if not tuned; PIV_AUTOTUNE=0 keeps the defaults). */
 int piv_xcorr_config(const piv_engine *e, int grid, int *windows_per_cta, int *threads_per_cta, float *tuned_ms);
 
-/* Correlation path of a grid.  PIV_XCORR_SIMT: register FFTs in FP32 on the CUDA cores
+/* Correlation path of a grid (0 = grid 1, 1 = grid 2).  PIV_XCORR_SIMT: register FFTs in FP32 on the CUDA cores
  * (default).  PIV_XCORR_TC_SPLIT: the transforms as DFT products on the tcgen05 tensor
  * cores with split-BF16 operands (hi*hi + hi*lo + lo*hi, FP32 accumulation).
  * PIV_XCORR_TC_BF16: one BF16 product per step (precision study only).  The tensor-core

@@ -999,8 +999,8 @@ int piv_debug_cc_planes(piv_engine *e, int grid, int first, int n, float *out)
 
 int piv_set_xcorr_path(piv_engine *e, int grid, int path)
 {
-    if (!e || (grid != 1 && grid != 2) || path < PIV_XCORR_SIMT || path > PIV_XCORR_TC_BF16) return PIV_ERR_ARG;
-    GridState &gs = e->grid[grid - 1];
+    if (!e || grid < 0 || grid > 1 || path < PIV_XCORR_SIMT || path > PIV_XCORR_TC_BF16) return PIV_ERR_ARG;
+    GridState &gs = e->grid[grid];
     if (path != PIV_XCORR_SIMT && !xcorr_tc_supported(gs.gg.ws_x, gs.gg.ws_y))
         return set_err(e, PIV_ERR_UNSUPPORTED, "window shape %dx%d has no tensor-core path", gs.gg.ws_x, gs.gg.ws_y);
     if (gs.path != path && e->graph) {
@@ -1014,8 +1014,8 @@ int piv_set_xcorr_path(piv_engine *e, int grid, int path)
 
 int piv_get_xcorr_path(const piv_engine *e, int grid, int *path)
 {
-    if (!e || (grid != 1 && grid != 2) || !path) return PIV_ERR_ARG;
-    *path = e->grid[grid - 1].path;
+    if (!e || grid < 0 || grid > 1 || !path) return PIV_ERR_ARG;
+    *path = e->grid[grid].path;
     return PIV_OK;
 }
 

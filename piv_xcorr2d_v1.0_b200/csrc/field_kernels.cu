@@ -42,12 +42,21 @@ __device__ __forceinline__ float deform_pixel(const DeformArgs &a, int idx, int 
     // aug_ex column i_x + hfws_x holds image column i_x - Nx_left -> padded-frame column
     const int c0 = i_x + col_off, r0 = i_y + row_off;
     float p[4];
+    if (c0 >= 0 && c0 + 1 < a.f2.cols && r0 >= 0 && r0 + 1 < a.f2.rows) {
+        // all four taps inside the padded frame (the common case): no per-tap checks
+        const uint8_t *q = a.f2.base + (size_t)r0 * a.f2.pitch + c0;
+        p[0] = (float)__ldg(q);
+        p[1] = (float)__ldg(q + 1);
+        p[2] = (float)__ldg(q + a.f2.pitch);
+        p[3] = (float)__ldg(q + a.f2.pitch + 1);
+    } else {
 #pragma unroll
-    for (int t = 0; t < 4; ++t) {
-        const int c = c0 + (t & 1), r = r0 + (t >> 1);
-        p[t] = (c >= 0 && c < a.f2.cols && r >= 0 && r < a.f2.rows)
-                   ? (float)__ldg(a.f2.base + (size_t)r * a.f2.pitch + c)
-                   : 0.f;
+        for (int t = 0; t < 4; ++t) {
+            const int c = c0 + (t & 1), r = r0 + (t >> 1);
+            p[t] = (c >= 0 && c < a.f2.cols && r >= 0 && r < a.f2.rows)
+                       ? (float)__ldg(a.f2.base + (size_t)r * a.f2.pitch + c)
+                       : 0.f;
+        }
     }
     ce1 = (1 - a_x) * (1 - a_y);
     ce2 = a_x * (1 - a_y);
@@ -56,10 +65,19 @@ __device__ __forceinline__ float deform_pixel(const DeformArgs &a, int idx, int 
     return ce1 * p[0] + ce2 * p[1] + ce3 * p[2] + ce4 * p[3];
 }
 
+// (v - st) / sp as the reference writes it; for a power-of-two spacing the reciprocal
+// is exact, and multiplying by it gives the identical correctly rounded quotient.
+template <bool POW2>
+__device__ __forceinline__ float cell_coord(float v, float st, float sp, float inv_sp)
+{
+    if constexpr (POW2) return (v - st) * inv_sp;
+    else return (v - st) / sp;
+}
+
 // Each thread writes 8 consecutive pixels of one row (two float4 stores).  When the
 // vector spacing and the field origin are multiples of 8 (the `cell8` launches), the 8
 // pixels lie in one cell of the field, so its 8 values are loaded once.
-template <bool CELL8>
+template <bool CELL8, bool POW2>
 __global__ void __launch_bounds__(256) deform_kernel(const DeformArgs a)
 {
     const int X0 = (blockIdx.x * blockDim.x + threadIdx.x) * 8;
@@ -67,15 +85,16 @@ __global__ void __launch_bounds__(256) deform_kernel(const DeformArgs a)
     if (X0 >= a.Nx_aug || Y >= a.Ny_aug) return;
     const float x_st_vec = (float)(a.hfws_x - a.sp_x * 3), y_st_vec = (float)(a.hfws_y - a.sp_y * 3);
     const float vsx = (float)a.sp_x, vsy = (float)a.sp_y;
+    const float ivx = 1.0f / vsx, ivy = 1.0f / vsy;
     const int col_off = a.f2.mx - a.Nx_left, row_off = a.f2.my - a.Ny_left;
 
-    float a_y = ((float)Y - y_st_vec) / vsy;
+    float a_y = cell_coord<POW2>((float)Y, y_st_vec, vsy, ivy);
     const int i_y = (int)floorf(a_y);
     a_y = a_y - (float)i_y;
 
     float res[8];
     if (CELL8) {
-        const int i_x = (int)floorf(((float)X0 - x_st_vec) / vsx);
+        const int i_x = (int)floorf(cell_coord<POW2>((float)X0, x_st_vec, vsx, ivx));
         const float u1 = ext_field(a.fx, a.Nx_vec, a.Ny_vec, i_x, i_y);
         const float u2 = ext_field(a.fx, a.Nx_vec, a.Ny_vec, i_x + 1, i_y);
         const float u3 = ext_field(a.fx, a.Nx_vec, a.Ny_vec, i_x, i_y + 1);
@@ -87,7 +106,7 @@ __global__ void __launch_bounds__(256) deform_kernel(const DeformArgs a)
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
             const int idx = X0 + q;
-            float a_x = ((float)idx - x_st_vec) / vsx;
+            float a_x = cell_coord<POW2>((float)idx, x_st_vec, vsx, ivx);
             a_x = a_x - (float)i_x;
             res[q] = deform_pixel(a, idx, Y, a_x, a_y, u1, u2, u3, u4, v1, v2, v3, v4, col_off, row_off);
         }
@@ -95,7 +114,7 @@ __global__ void __launch_bounds__(256) deform_kernel(const DeformArgs a)
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
             const int idx = X0 + q;
-            float a_x = ((float)idx - x_st_vec) / vsx;
+            float a_x = cell_coord<POW2>((float)idx, x_st_vec, vsx, ivx);
             const int i_x = (int)floorf(a_x);
             a_x = a_x - (float)i_x;
             res[q] = deform_pixel(a, idx, Y, a_x, a_y, ext_field(a.fx, a.Nx_vec, a.Ny_vec, i_x, i_y),
@@ -126,8 +145,14 @@ cudaError_t launch_deform(const DeformArgs &a, cudaStream_t s)
     // the run (its float quotient is exact for these small integers)
     const int x_st = a.hfws_x - a.sp_x * 3;
     const bool cell8 = (a.sp_x % 8 == 0) && (((x_st % 8) + 8) % 8 == 0);
-    if (cell8) deform_kernel<true><<<grid, block, 0, s>>>(a);
-    else deform_kernel<false><<<grid, block, 0, s>>>(a);
+    const bool pow2 = a.sp_x > 0 && a.sp_y > 0 && (a.sp_x & (a.sp_x - 1)) == 0 && (a.sp_y & (a.sp_y - 1)) == 0;
+    if (cell8) {
+        if (pow2) deform_kernel<true, true><<<grid, block, 0, s>>>(a);
+        else deform_kernel<true, false><<<grid, block, 0, s>>>(a);
+    } else {
+        if (pow2) deform_kernel<false, true><<<grid, block, 0, s>>>(a);
+        else deform_kernel<false, false><<<grid, block, 0, s>>>(a);
+    }
     return cudaGetLastError();
 }
 
