@@ -24,7 +24,8 @@
 //       W = C_a + i*C_b, inverse column FFT in registers.
 //   P4  row task (pair, row): inverse row FFT -> Re = corr_a, Im = corr_b;
 //       |.|/N written as fftshifted FP32 planes.
-//   P5  warp per window: 4-neighbour local maxima inside the search region,
+//   P5  warp per window (two warps for windows taller than 32 rows when the CTA has
+//       them): 4-neighbour local maxima inside the search region,
 //       count, register top-K (value desc, then lower index), 3-point Gaussian fit
 //       with an FP64 log-ratio denominator, predictor, limits, NaN/Inf removal.
 #pragma once
@@ -124,36 +125,23 @@ __device__ __forceinline__ void topk_insert(float (&tv)[K], int (&ti)[K], float 
 }
 
 // ------------------------------------------------------------------------------
-// Peak stage of one window (one warp): 4-neighbour local maxima inside the search
-// region, count, top-Npeak_save, 3-point Gaussian fit, predictor, limits, NaN/Inf
-// removal (find_local_max_2d, reduce_max_index_*, replace_local_max_2d,
-// peak_subpixel_4peak_2d, kernel_remove_nan).  P: the window's fftshifted plane in
-// shared memory with row stride WSX + 1.
+// Peak stage of one window: 4-neighbour local maxima inside the search region, count,
+// top-Npeak_save, 3-point Gaussian fit, predictor, limits, NaN/Inf removal
+// (find_local_max_2d, reduce_max_index_*, replace_local_max_2d, peak_subpixel_4peak_2d,
+// kernel_remove_nan).  P: the window's fftshifted plane in shared memory with row
+// stride WSX + 1.  One warp per window (peak_window), or, for windows of more than 32
+// rows, two warps that each scan half of the rows and merge their top-N through shared
+// memory (peak_window_part, then peak_window_merge after a barrier).
 // ------------------------------------------------------------------------------
+
+// Region rows first, first + step, ... scanned by this lane into its sorted top-K
+// (value desc, index asc); returns the lane's count of maxima.
 template <int WSX, int WSY, int K>
-__device__ __forceinline__ void peak_window(const XcorrArgs &a, const float *P, int w, int lane)
+__device__ __forceinline__ int peak_scan(const GridGeom &g, const float *P, int first, int step, float (&tv)[K],
+                                         int (&ti)[K])
 {
     constexpr int LDF = WSX + 1;
-    const GridGeom &g = a.g;
     const int rows = WSY - 2 * g.by;
-    if (a.cc_dump) {
-        // diagnostic mode: planes only, the pass outputs stay untouched
-        float *dst = a.cc_dump + (size_t)(w - a.w_first) * (WSX * WSY);
-        for (int t = lane; t < WSX * WSY; t += 32) {
-            const int j = t / WSX, i = t - j * WSX;
-            dst[t] = P[j * LDF + i];
-        }
-        return;
-    }
-    // the predictor of the window, fetched early (used by the Nps fitting lanes)
-    float pred_x = 0.f, pred_y = 0.f;
-    if (lane < g.Nps) {
-        pred_x = a.pred_x[w];
-        pred_y = a.pred_y[w];
-    }
-    // lane-local top-K of the lane's region rows, sorted (value desc, index asc)
-    float tv[K];
-    int ti[K];
 #pragma unroll
     for (int k = 0; k < K; ++k) {
         tv[k] = -1.f;
@@ -161,19 +149,20 @@ __device__ __forceinline__ void peak_window(const XcorrArgs &a, const float *P, 
     }
     // columns allowed by the border (and by the 4-neighbour stencil) as a bitmask
     constexpr int NWRD = (WSX + 31) / 32;
+    const int lo = g.bx > 1 ? g.bx : 1, hi = (WSX - 1 - g.bx) < (WSX - 2) ? (WSX - 1 - g.bx) : (WSX - 2);
     uint32_t allow[NWRD];
 #pragma unroll
     for (int q = 0; q < NWRD; ++q) {
-        uint32_t m = 0;
-#pragma unroll
-        for (int b = 0; b < 32; ++b) {
-            const int i = 32 * q + b;
-            m |= (uint32_t)((i >= 1) & (i <= WSX - 2) & (i >= g.bx) & (i <= WSX - 1 - g.bx)) << b;
-        }
-        allow[q] = m;
+        // bits [lo, hi] of word q
+        const int l = lo - 32 * q, h = hi - 32 * q;
+        const uint32_t upto = h >= 31 ? 0xffffffffu : (h < 0 ? 0u : ((2u << h) - 1u));
+        const uint32_t from = l <= 0 ? 0xffffffffu : (l > 31 ? 0u : ~((1u << l) - 1u));
+        allow[q] = upto & from;
     }
+    // v > 0 and v >= all four neighbours  <=>  v >= max(neighbours, smallest subnormal)
+    const float tiny = __int_as_float(1);
     int cnt = 0;
-    for (int jj = lane; jj < rows; jj += 32) {
+    for (int jj = first; jj < rows; jj += step) {
         const int j = g.by + jj;
         const float *pm = P + j * LDF;
         float mid[WSX];
@@ -185,9 +174,8 @@ __device__ __forceinline__ void peak_window(const XcorrArgs &a, const float *P, 
         for (int q = 0; q < NWRD; ++q) mk[q] = 0;
 #pragma unroll
         for (int i = 1; i < WSX - 1; ++i) {
-            const float v = mid[i];
-            const bool c = (v > 0.f) & (v >= mid[i - 1]) & (v >= mid[i + 1]) & (v >= pm[i - LDF]) & (v >= pm[i + LDF]);
-            mk[i >> 5] |= (uint32_t)c << (i & 31);
+            const float m = fmaxf(fmaxf(mid[i - 1], mid[i + 1]), fmaxf(fmaxf(pm[i - LDF], pm[i + LDF]), tiny));
+            mk[i >> 5] |= (uint32_t)(mid[i] >= m) << (i & 31);
         }
         // the row's maxima in column order into the lane's top-K
 #pragma unroll
@@ -201,16 +189,20 @@ __device__ __forceinline__ void peak_window(const XcorrArgs &a, const float *P, 
             }
         }
     }
-#pragma unroll
-    for (int off = 16; off >= 1; off >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, off);
-    // the window's top Nps: Nps rounds of a warp arg-max over the lanes' list heads.
-    // Candidates are positive, so their bit patterns order as unsigned integers: the
-    // largest value is one warp max-reduction, the lowest index holding it one
-    // min-reduction (the order of better()).  Indices are unique, so exactly one lane
-    // owns each winner and pops it.
-    float v = -1.f;
-    int idx = INT_MAX;
-    for (int k = 0; k < g.Nps; ++k) {
+    return cnt;
+}
+
+// Nps rounds of a warp arg-max over the lanes' list heads; lane k < Nps receives the
+// k-th best (value, index), -1 / INT_MAX when there are fewer candidates.  Candidates
+// are positive, so their bit patterns order as unsigned integers: the largest value
+// is one warp max-reduction, the lowest index holding it one min-reduction (the order
+// of better()).  Indices are unique, so exactly one lane owns each winner and pops it.
+template <int K>
+__device__ __forceinline__ void peak_select(int Nps, int lane, float (&tv)[K], int (&ti)[K], float &v, int &idx)
+{
+    v = -1.f;
+    idx = INT_MAX;
+    for (int k = 0; k < Nps; ++k) {
         const uint32_t key = tv[0] > 0.f ? __float_as_uint(tv[0]) : 0u;
         const uint32_t kmax = __reduce_max_sync(0xffffffffu, key);
         const uint32_t imin = __reduce_min_sync(0xffffffffu, key == kmax ? (uint32_t)ti[0] : 0xffffffffu);
@@ -230,6 +222,16 @@ __device__ __forceinline__ void peak_window(const XcorrArgs &a, const float *P, 
             ti[K - 1] = INT_MAX;
         }
     }
+}
+
+// Sub-pixel fit of the candidate held by lane (< Nps), limits, NaN/Inf removal and the
+// stores of the window's outputs; cnt is the window's count of maxima.
+template <int WSX, int WSY>
+__device__ __forceinline__ void peak_fit_store(const XcorrArgs &a, const float *P, int w, int lane, float v, int idx,
+                                               int cnt, float pred_x, float pred_y)
+{
+    constexpr int LDF = WSX + 1;
+    const GridGeom &g = a.g;
     if (lane < g.Nps) {
         float ox = 0.f, oy = 0.f;
         bool ok = false;
@@ -268,6 +270,100 @@ __device__ __forceinline__ void peak_window(const XcorrArgs &a, const float *P, 
         a.pval[o] = (v > 0.f) ? v : 0.f;
     }
     if (lane == 0) a.count[w] = cnt;
+}
+
+// diagnostic mode: the plane only, the pass outputs stay untouched
+template <int WSX, int WSY>
+__device__ __forceinline__ void peak_dump(const XcorrArgs &a, const float *P, int w, int lane)
+{
+    constexpr int LDF = WSX + 1;
+    float *dst = a.cc_dump + (size_t)(w - a.w_first) * (WSX * WSY);
+    for (int t = lane; t < WSX * WSY; t += 32) {
+        const int j = t / WSX, i = t - j * WSX;
+        dst[t] = P[j * LDF + i];
+    }
+}
+
+__device__ __forceinline__ int warp_sum(int x)
+{
+    return __reduce_add_sync(0xffffffffu, x);
+}
+
+// One warp per window.
+template <int WSX, int WSY, int K>
+__device__ __forceinline__ void peak_window(const XcorrArgs &a, const float *P, int w, int lane)
+{
+    if (a.cc_dump) {
+        peak_dump<WSX, WSY>(a, P, w, lane);
+        return;
+    }
+    // the predictor of the window, fetched early (used by the Nps fitting lanes)
+    float pred_x = 0.f, pred_y = 0.f;
+    if (lane < a.g.Nps) {
+        pred_x = a.pred_x[w];
+        pred_y = a.pred_y[w];
+    }
+    float tv[K];
+    int ti[K];
+    const int cnt = warp_sum(peak_scan<WSX, WSY, K>(a.g, P, lane, 32, tv, ti));
+    float v;
+    int idx;
+    peak_select<K>(a.g.Nps, lane, tv, ti, v, idx);
+    peak_fit_store<WSX, WSY>(a, P, w, lane, v, idx, cnt, pred_x, pred_y);
+}
+
+// Two warps per window: one warp's half of the rows and its top-Nps.
+struct PeakPart {
+    float v[8];
+    int idx[8];
+    int cnt;
+};
+
+template <int WSX, int WSY, int K>
+__device__ __forceinline__ void peak_window_part(const XcorrArgs &a, const float *P, int part, int lane,
+                                                 PeakPart &out)
+{
+    if (a.cc_dump) return;
+    float tv[K];
+    int ti[K];
+    const int cnt = warp_sum(peak_scan<WSX, WSY, K>(a.g, P, 32 * part + lane, 64, tv, ti));
+    float v;
+    int idx;
+    peak_select<K>(a.g.Nps, lane, tv, ti, v, idx);
+    if (lane < a.g.Nps) {
+        out.v[lane] = v;
+        out.idx[lane] = idx;
+    }
+    if (lane == 0) out.cnt = cnt;
+}
+
+// After a barrier, one warp merges the two halves' top-Nps (one entry per lane) and fits.
+template <int WSX, int WSY>
+__device__ __forceinline__ void peak_window_merge(const XcorrArgs &a, const float *P, int w, int lane,
+                                                  const PeakPart (&parts)[2])
+{
+    if (a.cc_dump) {
+        peak_dump<WSX, WSY>(a, P, w, lane);
+        return;
+    }
+    const int Nps = a.g.Nps;
+    float pred_x = 0.f, pred_y = 0.f;
+    if (lane < Nps) {
+        pred_x = a.pred_x[w];
+        pred_y = a.pred_y[w];
+    }
+    float tv[1] = {-1.f};
+    int ti[1] = {INT_MAX};
+    if (lane < 2 * Nps) {
+        const PeakPart &pp = parts[lane >= Nps];
+        const int k = lane >= Nps ? lane - Nps : lane;
+        tv[0] = pp.v[k];
+        ti[0] = pp.idx[k];
+    }
+    float v;
+    int idx;
+    peak_select<1>(Nps, lane, tv, ti, v, idx);
+    peak_fit_store<WSX, WSY>(a, P, w, lane, v, idx, parts[0].cnt + parts[1].cnt, pred_x, pred_y);
 }
 
 template <int WSX, int WSY, int B, int NT, int K, bool DEF>
@@ -380,14 +476,27 @@ __global__ void __launch_bounds__(NT) xcorr_peak_kernel(const XcorrArgs a)
     }
     __syncthreads();
 
-    // ---------------- P5: peaks, warp per window ----------------
+    // ---------------- P5: peaks, warp per window (two for tall windows) ----------------
     const int warp = tid >> 5, lane = tid & 31;
     constexpr int NW = NT / 32;
-    for (int b = warp; b < B; b += NW) {
+    if constexpr (WSY > 32 && NW >= 2 * B) {
+        // the even window buffers are free after P4: the halves' results go there
+        static_assert(B * sizeof(PeakPart[2]) <= WIN * sizeof(float2), "peak scratch fits in window buffer 0");
+        PeakPart(*parts)[2] = reinterpret_cast<PeakPart(*)[2]>(sm);
+        const int b = warp >> 1, part = warp & 1;
         const int w = w_base + b;
-        if (w >= a.w_end) continue;
+        const bool live = b < B && w < a.w_end;
         const float *P = reinterpret_cast<const float *>(sm + ((b & ~1) + 1) * WIN) + (b & 1) * (WSY * LDF);
-        peak_window<WSX, WSY, K>(a, P, w, lane);
+        if (live) peak_window_part<WSX, WSY, K>(a, P, part, lane, parts[b][part]);
+        __syncthreads();
+        if (live && part == 0) peak_window_merge<WSX, WSY>(a, P, w, lane, parts[b]);
+    } else {
+        for (int b = warp; b < B; b += NW) {
+            const int w = w_base + b;
+            if (w >= a.w_end) continue;
+            const float *P = reinterpret_cast<const float *>(sm + ((b & ~1) + 1) * WIN) + (b & 1) * (WSY * LDF);
+            peak_window<WSX, WSY, K>(a, P, w, lane);
+        }
     }
 }
 

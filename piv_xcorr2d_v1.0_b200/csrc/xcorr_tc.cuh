@@ -363,10 +363,22 @@ __global__ void __launch_bounds__(TcShape<WS>::THREADS, 1) xcorr_tc_kernel(const
             }
         }
 
-        // ---- peaks: warp per window ----
-        for (int b = wq; b < NWIN; b += 4) {
+        // ---- peaks: warp per window; two warps per 64-row window ----
+        if constexpr (WS > 32) {
+            static_assert(NWIN * 2 == 4, "two warps per window");
+            static_assert((size_t)NWIN * WS * LDF * 4 + NWIN * sizeof(PeakPart[2]) <= 2 * A_BYTES, "peak scratch");
+            PeakPart(*parts)[2] = reinterpret_cast<PeakPart(*)[2]>(planes + NWIN * WS * LDF);
+            const int b = wq >> 1, part = wq & 1;
             const int wb = a.w_first + tile * NWIN + b;
-            if (wb < a.w_end) peak_window<WS, WS, K>(a, planes + b * (WS * LDF), wb, lane);
+            const float *P = planes + b * (WS * LDF);
+            if (wb < a.w_end) peak_window_part<WS, WS, K>(a, P, part, lane, parts[b][part]);
+            tc::named_sync(bar_id, 128);
+            if (wb < a.w_end && part == 0) peak_window_merge<WS, WS>(a, P, wb, lane, parts[b]);
+        } else {
+            for (int b = wq; b < NWIN; b += 4) {
+                const int wb = a.w_first + tile * NWIN + b;
+                if (wb < a.w_end) peak_window<WS, WS, K>(a, planes + b * (WS * LDF), wb, lane);
+            }
         }
         tc::named_sync(bar_id, 128);  // planes (aliasing the operand buffers) are consumed
     }
