@@ -11,8 +11,9 @@ pair: 113,300 (412 x 275).
 
   value  device-resident: frames already in HBM, CUDA events on the engine stream around
          each replay of the captured pair graph; L2 flushed before every step.
-  e2e    through the C-ABI with host buffers: upload of both frames from pinned memory,
-         the pair, readback of the filtered grid-2 field, every step.
+  e2e    through the C-ABI with host buffers: upload of both frames from pinned memory
+         (piv_queue_images, so the upload of pair k+1 overlaps the computation of pair
+         k), the pair, readback of the filtered grid-2 field, every step.
   --impl reference  the reference's own engine (xcorr2d_multi + mhe_gpu, compiled for
          sm_100a from its sources) on the same pair through its public methods.
 
@@ -190,14 +191,19 @@ def run_ours(args, rank, world, local):
         R.barrier(world)
         ms = [starts[k].elapsed_time(ends[k]) for k in range(args.steps)]
 
-        # end to end through the C-ABI with host buffers (pinned frames in, field out)
-        e.set_device_images(0, 0)
+        # end to end through the C-ABI with host buffers: every step uploads its pair
+        # from pinned memory (piv_queue_images: the upload of pair k+1 overlaps pair k)
+        # and reads its filtered field back
+        e.queue_images(h1.ctypes.data, h2.ctypes.data)
         e.run_pair()
         e.field(3)
         R.barrier(world)
         t0 = time.perf_counter()
-        for _ in range(args.steps):
+        e.queue_images(h1.ctypes.data, h2.ctypes.data)
+        for k in range(args.steps):
             e.run_pair()
+            if k + 1 < args.steps:
+                e.queue_images(h1.ctypes.data, h2.ctypes.data)
             _, _, dx, dy, vv = e.field(3)
         e2e_local = time.perf_counter() - t0
     total_s = R.max_over_ranks(sum(ms) / 1e3, world)

@@ -138,6 +138,18 @@ int piv_set_images(piv_engine *e, const uint8_t *f1, const uint8_t *f2, size_t p
  * valid until piv_prep has run. NULL, NULL switches back to the host buffers. */
 int piv_set_device_images(piv_engine *e, const uint8_t *d_f1, const uint8_t *d_f2);
 
+/* Pipelined input (no counterpart in the reference, whose main loop uploads a pair and
+ * then computes it): queues the upload of the next pair's frames (Nx*Ny bytes each,
+ * row-major host memory; pinned memory lets the copy overlap) into one of two device
+ * input slots on the engine's copy stream and returns at once.  The next piv_run_pair
+ * computes that pair, after the upload, while the caller may already queue the pair
+ * after it: the upload of pair k+1 then overlaps the computation of pair k.  A slot is
+ * refilled only after the pair that read it has finished.  PIV_ERR_STATE if a queued
+ * pair has not been run yet; piv_set_images / piv_set_device_images discard a queued
+ * pair.  The host buffers must stay valid until the upload is done (piv_run_pair of
+ * that pair returned and its results were read, or piv_synchronize). */
+int piv_queue_images(piv_engine *e, const uint8_t *f1, const uint8_t *f2);
+
 /* prep_img_data (X/xcorr2d_multi_grid.cu:1271-1282) fused with the optional MHE of
  * both frames (X/main.cpp:267-283, mhe_gpu::processsing): uploads the frames (one
  * asynchronous copy per frame from the pinned buffers, or a device-to-device copy),

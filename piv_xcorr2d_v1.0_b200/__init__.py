@@ -140,6 +140,7 @@ EXPORTS = {
     "piv_kernel_launches_per_pair": (C.c_int, [_P, C.POINTER(C.c_int)]),
     "piv_time_stage": (C.c_int, [_P, C.c_int, C.c_int, _F]),
     "piv_probe_fp32_peak": (C.c_int, [_F]),
+    "piv_queue_images": (C.c_int, [_P, _P, _P]),
     "piv_set_xcorr_path": (C.c_int, [_P, C.c_int, C.c_int]),
     "piv_get_xcorr_path": (C.c_int, [_P, C.c_int, C.POINTER(C.c_int)]),
     "piv_tc_gemm_check": (C.c_int, [_F, _F, _F, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]),
@@ -173,6 +174,17 @@ class PivError(RuntimeError):
     def __init__(self, status, msg):
         super().__init__(f"[{status}] {msg}")
         self.status = status
+
+
+def _addr(a, nbytes):
+    """Address of a C-contiguous host buffer of at least nbytes (numpy array or a CPU
+    torch tensor)."""
+    if hasattr(a, "data_ptr"):
+        assert a.is_contiguous() and a.numel() * a.element_size() >= nbytes and not a.is_cuda
+        return a.data_ptr()
+    a = np.asarray(a)
+    assert a.flags.c_contiguous and a.nbytes >= nbytes
+    return a.ctypes.data
 
 
 def _ptr(a, ct):
@@ -311,6 +323,14 @@ class Engine:
     def set_device_images(self, d1: int, d2: int):
         self._ck(lib().piv_set_device_images(self.h, C.c_void_p(d1), C.c_void_p(d2)))
 
+    def queue_images(self, f1, f2):
+        """Queues the upload of the next pair (host arrays or host addresses; pinned memory
+        overlaps the copy with the pair in flight).  The arrays must stay alive and
+        unchanged until that pair has been run and its results read."""
+        a1 = f1 if isinstance(f1, int) else _addr(f1, self.p.Nx * self.p.Ny)
+        a2 = f2 if isinstance(f2, int) else _addr(f2, self.p.Nx * self.p.Ny)
+        self._ck(lib().piv_queue_images(self.h, C.c_void_p(a1), C.c_void_p(a2)))
+
     # -- stages --
     def prep(self):
         self._ck(lib().piv_prep(self.h))
@@ -351,9 +371,9 @@ class Engine:
 
     def field(self, selection):
         """(x, y, dx, dy, valid); raw selections (0, 2) give [Nt, Npeak_save] candidate arrays."""
-        g = selection // 2
+        g = 0 if selection < 2 else 1
         nt = self._nt(g)
-        raw = selection % 2 == 0
+        raw = selection in (0, 2)
         n = nt * self.p.Npeak_save if raw else nt
         x = np.empty(nt, np.float32)
         y = np.empty(nt, np.float32)

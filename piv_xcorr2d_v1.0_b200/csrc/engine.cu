@@ -142,8 +142,21 @@ struct piv_engine {
     int *d_status = nullptr, *d_list_n = nullptr;
     int *h_status = nullptr;
     bool prepared = false;
-    cudaGraphExec_t graph = nullptr;
-    const uint8_t *graph_in1 = nullptr, *graph_in2 = nullptr;
+    // captured pair graphs, one per input-frame address pair (the host path, caller
+    // frames, and the two upload slots each get their own)
+    struct PairGraph {
+        cudaGraphExec_t exec = nullptr;
+        const uint8_t *in1 = nullptr, *in2 = nullptr;
+    };
+    PairGraph graphs[4];
+    int n_graphs = 0;
+    // pipelined input (piv_queue_images): two device slots filled on the copy stream;
+    // ev_up[s] marks slot s uploaded, ev_done[s] the end of the last pair that read it
+    cudaStream_t copy_stream = nullptr;
+    uint8_t *d_slot[2][2] = {};
+    cudaEvent_t ev_up[2] = {}, ev_done[2] = {};
+    bool slot_read[2] = {};
+    int next_slot = 0, pending_slot = -1, reading_slot = -1;
     std::string err;
     bool timing = false;
     cudaEvent_t ev[6] = {};
@@ -192,7 +205,15 @@ int dalloc(piv_engine *e, T **ptr, size_t n)
 
 void free_all(piv_engine *e)
 {
-    if (e->graph) cudaGraphExecDestroy(e->graph);
+    for (int i = 0; i < e->n_graphs; ++i) cudaGraphExecDestroy(e->graphs[i].exec);
+    e->n_graphs = 0;
+    for (int q = 0; q < 2; ++q) {
+        cudaFree(e->d_slot[q][0]);
+        cudaFree(e->d_slot[q][1]);
+        if (e->ev_up[q]) cudaEventDestroy(e->ev_up[q]);
+        if (e->ev_done[q]) cudaEventDestroy(e->ev_done[q]);
+    }
+    if (e->copy_stream) cudaStreamDestroy(e->copy_stream);
     cudaFreeHost(e->h_f1);
     cudaFreeHost(e->h_f2);
     cudaFreeHost(e->h_status);
@@ -734,6 +755,33 @@ int piv_set_images(piv_engine *e, const uint8_t *f1, const uint8_t *f2, size_t p
         std::memcpy(e->h_f2 + j * Nx, f2 + j * pitch, Nx);
     }
     e->d_in1 = e->d_in2 = nullptr;
+    e->pending_slot = -1;
+    return PIV_OK;
+}
+
+int piv_queue_images(piv_engine *e, const uint8_t *f1, const uint8_t *f2)
+{
+    if (!e || !f1 || !f2) return PIV_ERR_ARG;
+    if (e->pending_slot >= 0) return set_err(e, PIV_ERR_STATE, "a queued pair has not been run yet");
+    cudaSetDevice(e->device);
+    const size_t npix = (size_t)e->p.Nx * e->p.Ny;
+    if (!e->copy_stream) {
+        CK(cudaStreamCreateWithFlags(&e->copy_stream, cudaStreamNonBlocking));
+        for (int q = 0; q < 2; ++q) {
+            int rc;
+            if ((rc = dalloc(e, &e->d_slot[q][0], npix)) || (rc = dalloc(e, &e->d_slot[q][1], npix))) return rc;
+            CK(cudaEventCreateWithFlags(&e->ev_up[q], cudaEventDisableTiming));
+            CK(cudaEventCreateWithFlags(&e->ev_done[q], cudaEventDisableTiming));
+        }
+    }
+    const int q = e->next_slot;
+    // the slot's previous pair must have finished reading it
+    if (e->slot_read[q]) CK(cudaStreamWaitEvent(e->copy_stream, e->ev_done[q], 0));
+    CK(cudaMemcpyAsync(e->d_slot[q][0], f1, npix, cudaMemcpyHostToDevice, e->copy_stream));
+    CK(cudaMemcpyAsync(e->d_slot[q][1], f2, npix, cudaMemcpyHostToDevice, e->copy_stream));
+    CK(cudaEventRecord(e->ev_up[q], e->copy_stream));
+    e->pending_slot = q;
+    e->next_slot = q ^ 1;
     return PIV_OK;
 }
 
@@ -742,6 +790,7 @@ int piv_set_device_images(piv_engine *e, const uint8_t *d_f1, const uint8_t *d_f
     if (!e || (!d_f1) != (!d_f2)) return PIV_ERR_ARG;
     e->d_in1 = d_f1;
     e->d_in2 = d_f2;
+    e->pending_slot = -1;
     return PIV_OK;
 }
 
@@ -816,11 +865,24 @@ int piv_run_pair(piv_engine *e)
         e->have_times = true;
         return PIV_OK;
     }
-    if (e->graph && (e->graph_in1 != e->d_in1 || e->graph_in2 != e->d_in2)) {
-        cudaGraphExecDestroy(e->graph);
-        e->graph = nullptr;
+    // a queued upload (piv_queue_images) becomes this pair's input
+    if (e->pending_slot >= 0) {
+        const int q = e->pending_slot;
+        CK(cudaStreamWaitEvent(e->stream, e->ev_up[q], 0));
+        e->d_in1 = e->d_slot[q][0];
+        e->d_in2 = e->d_slot[q][1];
+        e->reading_slot = q;
+        e->pending_slot = -1;
     }
-    if (!e->graph) {
+    piv_engine::PairGraph *pg = nullptr;
+    for (int i = 0; i < e->n_graphs; ++i)
+        if (e->graphs[i].in1 == e->d_in1 && e->graphs[i].in2 == e->d_in2) pg = &e->graphs[i];
+    if (!pg) {
+        if (e->n_graphs == 4) {  // drop the oldest
+            cudaGraphExecDestroy(e->graphs[0].exec);
+            for (int i = 1; i < 4; ++i) e->graphs[i - 1] = e->graphs[i];
+            e->n_graphs = 3;
+        }
         cudaGraph_t g = nullptr;
         CK(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
         rc = do_pair(e, false);
@@ -830,16 +892,20 @@ int piv_run_pair(piv_engine *e)
             return rc;
         }
         if (ce != cudaSuccess) return set_err(e, PIV_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(ce));
-        cudaError_t ie = cudaGraphInstantiate(&e->graph, g, 0);
+        cudaGraphExec_t exec = nullptr;
+        cudaError_t ie = cudaGraphInstantiate(&exec, g, 0);
         cudaGraphDestroy(g);
-        if (ie != cudaSuccess) {
-            e->graph = nullptr;
-            return set_err(e, PIV_ERR_CUDA, "graph instantiation failed: %s", cudaGetErrorString(ie));
-        }
-        e->graph_in1 = e->d_in1;
-        e->graph_in2 = e->d_in2;
+        if (ie != cudaSuccess) return set_err(e, PIV_ERR_CUDA, "graph instantiation failed: %s", cudaGetErrorString(ie));
+        pg = &e->graphs[e->n_graphs++];
+        pg->exec = exec;
+        pg->in1 = e->d_in1;
+        pg->in2 = e->d_in2;
     }
-    CK(cudaGraphLaunch(e->graph, e->stream));
+    CK(cudaGraphLaunch(pg->exec, e->stream));
+    if (e->reading_slot >= 0 && e->d_in1 == e->d_slot[e->reading_slot][0]) {
+        CK(cudaEventRecord(e->ev_done[e->reading_slot], e->stream));
+        e->slot_read[e->reading_slot] = true;
+    }
     e->prepared = true;
     e->grid[0].has_pass = e->p.Npass1 > 0;
     e->grid[0].last_deformed = e->p.Npass1 > 1;
@@ -1003,10 +1069,10 @@ int piv_set_xcorr_path(piv_engine *e, int grid, int path)
     GridState &gs = e->grid[grid];
     if (path != PIV_XCORR_SIMT && !xcorr_tc_supported(gs.gg.ws_x, gs.gg.ws_y))
         return set_err(e, PIV_ERR_UNSUPPORTED, "window shape %dx%d has no tensor-core path", gs.gg.ws_x, gs.gg.ws_y);
-    if (gs.path != path && e->graph) {
+    if (gs.path != path && e->n_graphs) {
         cudaStreamSynchronize(e->stream);
-        cudaGraphExecDestroy(e->graph);
-        e->graph = nullptr;
+        for (int i = 0; i < e->n_graphs; ++i) cudaGraphExecDestroy(e->graphs[i].exec);
+        e->n_graphs = 0;
     }
     gs.path = path;
     return PIV_OK;
