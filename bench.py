@@ -61,9 +61,28 @@ def workload_params(P, device_id=0, Ny=NY):
                             insert_threshold_p1=2.0, insert_threshold_p2=2.0)
 
 
+def workload_synth(P, seed=1):
+    return P.synth_params(NX, NY, ppp=0.04, sigma=0.6, field=P.PIV_FIELD_VORTEX, a=10.0, b=600.0, c=0.002, seed=seed)
+
+
 def workload_pair(P, seed=1):
-    s = P.synth_params(NX, NY, ppp=0.04, sigma=0.6, field=P.PIV_FIELD_VORTEX, a=10.0, b=600.0, c=0.002, seed=seed)
-    return P.synth_pair(s)
+    return P.synth_pair(workload_synth(P, seed))
+
+
+def accuracy(P, e, s):
+    """The filtered grid-2 field against the known synthetic displacement u(x_g) at the
+    vector positions: RMS over valid vectors (all, and away from the image border by two
+    vector spacings), and the valid fraction."""
+    x, y, dx, dy, v = e.field(3)
+    u, w = P.synth_field(s, x, y)
+    ok = v == 1
+    err = np.hypot(dx - u, dy - w)
+    sp = e.p.spacing_x2
+    inner = ok & (x > 2 * sp) & (x < NX - 2 * sp) & (y > 2 * sp) & (y < NY - 2 * sp)
+    return {"rms_px": round(float(np.sqrt(np.mean(err[ok] ** 2))), 4),
+            "rms_interior_px": round(float(np.sqrt(np.mean(err[inner] ** 2))), 4),
+            "valid_frac": round(float(ok.mean()), 4),
+            "truth": "u(x_g) of the generator's Lamb-Oseen vortex + shear at the vector positions"}
 
 
 def fft_flops(wsx, wsy):
@@ -212,6 +231,8 @@ def run_ours(args, rank, world, local):
     e2e = {"value": R.sum_over_ranks(args.steps * nvec, world) / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 2 * NX * NY,
            "d2h_bytes_per_step": int(dx.nbytes + dy.nbytes + vv.nbytes)}
 
+    acc = accuracy(P, e, workload_synth(P, seed=1 + rank))
+
     # live roofline of the dominant kernel (grid-2 correlation), on the engine stream
     e.set_device_images(d1.data_ptr(), d2.data_ptr())
     e.run_pair()
@@ -237,6 +258,7 @@ def run_ours(args, rank, world, local):
                    "vectors_per_pair": nvec, "pairs_per_step_per_gpu": 1, "parallelism": f"replicas x{world}",
                    "l2": "flushed (512 MB write) before every timed step", "xcorr_autotune": tuned},
         "e2e": e2e, "roofline": roofline, "gpu_launches": launches, "clocks": clk.summary(),
+        "accuracy": acc,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(P, f1, f2, args.cpu_rows)

@@ -150,6 +150,11 @@ int piv_set_device_images(piv_engine *e, const uint8_t *d_f1, const uint8_t *d_f
  * that pair returned and its results were read, or piv_synchronize). */
 int piv_queue_images(piv_engine *e, const uint8_t *f1, const uint8_t *f2);
 
+/* Page-locked host memory for the frames a caller feeds to piv_queue_images (uploads
+ * from it overlap the computation); release with piv_host_free. */
+int piv_host_alloc(size_t bytes, void **ptr);
+int piv_host_free(void *ptr);
+
 /* prep_img_data (X/xcorr2d_multi_grid.cu:1271-1282) fused with the optional MHE of
  * both frames (X/main.cpp:267-283, mhe_gpu::processsing): uploads the frames (one
  * asynchronous copy per frame from the pinned buffers, or a device-to-device copy),

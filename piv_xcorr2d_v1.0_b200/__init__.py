@@ -141,6 +141,8 @@ EXPORTS = {
     "piv_time_stage": (C.c_int, [_P, C.c_int, C.c_int, _F]),
     "piv_probe_fp32_peak": (C.c_int, [_F]),
     "piv_queue_images": (C.c_int, [_P, _P, _P]),
+    "piv_host_alloc": (C.c_int, [C.c_size_t, C.POINTER(_P)]),
+    "piv_host_free": (C.c_int, [_P]),
     "piv_set_xcorr_path": (C.c_int, [_P, C.c_int, C.c_int]),
     "piv_get_xcorr_path": (C.c_int, [_P, C.c_int, C.POINTER(C.c_int)]),
     "piv_tc_gemm_check": (C.c_int, [_F, _F, _F, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]),

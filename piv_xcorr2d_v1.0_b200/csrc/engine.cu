@@ -470,9 +470,23 @@ int do_pair(piv_engine *e, bool with_events)
 // The autotuner: every instantiated variant (windows per CTA, threads per CTA) of each
 // grid's window shape is timed on this engine's own geometry, with the frames (and the
 // deformed frame, the mode most passes run in) holding a particle-like pattern; the
-// fastest variant is kept.  PIV_AUTOTUNE=0 keeps the defaults.
+// fastest variant is kept.  PIV_AUTOTUNE=0 keeps the defaults; PIV_XCORR_VARIANT=v1,v2
+// fixes the variants by index.
 int tune_xcorr(piv_engine *e)
 {
+    if (const char *fixed = getenv("PIV_XCORR_VARIANT")) {
+        // "v1,v2": the grids' variants by index, no timing (profiling a chosen variant)
+        int v[2] = {0, 0};
+        if (sscanf(fixed, "%d,%d", &v[0], &v[1]) != 2) return set_err(e, PIV_ERR_ARG, "PIV_XCORR_VARIANT wants v1,v2");
+        for (int k = 0; k < 2; ++k) {
+            GridState &gs = e->grid[k];
+            if (v[k] < 0 || v[k] >= xcorr_variants(gs.gg.ws_x, gs.gg.ws_y))
+                return set_err(e, PIV_ERR_ARG, "PIV_XCORR_VARIANT: grid %d has %d variants", k + 1,
+                               xcorr_variants(gs.gg.ws_x, gs.gg.ws_y));
+            gs.variant = v[k];
+        }
+        return PIV_OK;
+    }
     const char *env = getenv("PIV_AUTOTUNE");
     if (env && atoi(env) == 0) return PIV_OK;
     const piv_params &p = e->p;
@@ -783,6 +797,19 @@ int piv_queue_images(piv_engine *e, const uint8_t *f1, const uint8_t *f2)
     e->pending_slot = q;
     e->next_slot = q ^ 1;
     return PIV_OK;
+}
+
+int piv_host_alloc(size_t bytes, void **ptr)
+{
+    if (!ptr || bytes == 0) return PIV_ERR_ARG;
+    *ptr = nullptr;
+    return cudaHostAlloc(ptr, bytes, cudaHostAllocDefault) == cudaSuccess ? PIV_OK : PIV_ERR_ALLOC;
+}
+
+int piv_host_free(void *ptr)
+{
+    if (!ptr) return PIV_OK;
+    return cudaFreeHost(ptr) == cudaSuccess ? PIV_OK : PIV_ERR_CUDA;
 }
 
 int piv_set_device_images(piv_engine *e, const uint8_t *d_f1, const uint8_t *d_f2)

@@ -10,8 +10,9 @@
 // filtered and median-only) into the result folder, which is created if missing.
 // Messages follow the reference's; exit status 0 = "NO ERROR!", 1 = "ERROR!".
 //
-// --overlap: reads the next pair's frames and writes the previous pair's files on host
-// threads while the GPU processes the current pair.
+// --overlap: while the GPU processes the current pair, reads the next pair's frames into
+// a second pinned buffer pair and queues their upload (piv_queue_images, overlapping the
+// computation), and writes the previous pair's files on a host thread.
 // --resume:  skips pairs whose output files all exist already.
 // --npy:     also writes every field as a float32 .npy sidecar next to its .dat file
 //            ([Ny_vec][Nx_vec][2] filtered, [Ny_vec][Nx_vec][Npeak_save][2] raw).
@@ -215,10 +216,22 @@ int main(int argc, char **argv)
     }
     piv_geometry g;
     piv_get_geometry(e, &g);
-    uint8_t *h1 = nullptr, *h2 = nullptr;
-    piv_host_images(e, &h1, &h2);
     const size_t npx = (size_t)p.Nx * p.Ny;
-    std::vector<uint8_t> next1(npx), next2(npx);
+    // frame buffers: two pinned pairs (the engine's own and one more) so that in --overlap
+    // mode the next pair is read while the current one is computed, then its upload is
+    // queued (piv_queue_images) while the GPU still works
+    uint8_t *hb[2][2] = {};
+    piv_host_images(e, &hb[0][0], &hb[0][1]);
+    void *extra1 = nullptr, *extra2 = nullptr;
+    if (overlap && (piv_host_alloc(npx, &extra1) || piv_host_alloc(npx, &extra2))) {
+        printf("cudaMallocHost ERROR!\n");
+        piv_host_free(extra1);
+        piv_destroy(e);
+        return 1;
+    }
+    hb[1][0] = static_cast<uint8_t *>(extra1);
+    hb[1][1] = static_cast<uint8_t *>(extra2);
+    std::vector<uint8_t> next1(overlap ? 0 : npx), next2(overlap ? 0 : npx);
     bool status = true;
     std::thread writer;
     int writer_rc = 0;
@@ -232,7 +245,13 @@ int main(int argc, char **argv)
         return r ? r : piv_tiff_read8(p2.c_str(), b, p.Nx, p.Ny);
     };
 
-    int have_next = read_pair(pairs[0], next1.data(), next2.data()) == PIV_OK ? 1 : -1;
+    int have_next;
+    if (overlap) {
+        have_next = read_pair(pairs[0], hb[0][0], hb[0][1]) == PIV_OK ? 1 : -1;
+        if (have_next > 0 && (rc = piv_queue_images(e, hb[0][0], hb[0][1]))) have_next = -1;
+    } else {
+        have_next = read_pair(pairs[0], next1.data(), next2.data()) == PIV_OK ? 1 : -1;
+    }
     for (size_t i = 0; i < pairs.size(); ++i) {
         auto begin = std::chrono::steady_clock::now();
         printf("Processing pair %d: %zu out of %zu\n", pairs[i], i + 1, pairs.size());
@@ -241,23 +260,22 @@ int main(int argc, char **argv)
             status = false;
             break;
         }
-        if ((rc = piv_set_images(e, next1.data(), next2.data(), 0)) || (rc = piv_run_pair(e))) {
+        if ((!overlap && (rc = piv_set_images(e, next1.data(), next2.data(), 0))) || (rc = piv_run_pair(e))) {
             printf("xcor pair processing failed: %s\n", piv_last_error(e));
             status = false;
             break;
         }
-        // while the GPU works: read the next pair's frames
-        std::thread reader;
+        // while the GPU works: read the next pair's frames and queue their upload
         int next_rc = 0;
-        if (i + 1 < pairs.size()) {
-            if (overlap) {
-                reader = std::thread([&, idx = pairs[i + 1]] { next_rc = read_pair(idx, next1.data(), next2.data()); });
-            }
+        if (i + 1 < pairs.size() && overlap) {
+            // the other buffer pair fed pair i-1, whose upload finished before it ran
+            uint8_t *a = hb[(i + 1) & 1][0], *b = hb[(i + 1) & 1][1];
+            next_rc = read_pair(pairs[i + 1], a, b);
+            if (next_rc == PIV_OK) next_rc = piv_queue_images(e, a, b);
         }
         PairOutput out;
         out.idx = pairs[i];
         rc = fetch(e, p, g, out);
-        if (reader.joinable()) reader.join();
         if (i + 1 < pairs.size() && !overlap) next_rc = read_pair(pairs[i + 1], next1.data(), next2.data());
         have_next = next_rc == PIV_OK ? 1 : -1;
         if (rc) {
@@ -288,6 +306,8 @@ int main(int argc, char **argv)
         if (writer_rc) status = false;
     }
     piv_destroy(e);
+    piv_host_free(extra1);
+    piv_host_free(extra2);
     printf(status ? "NO ERROR!\n" : "ERROR!\n");
     return status ? 0 : 1;
 }

@@ -180,3 +180,53 @@ def test_bf16_single_product_precision(cuda, ws, sp):
         worst = max(worst, np.abs(got[w] - want).max() / max(want.max(), 1.0))
     print(f"tc bf16x1 {ws}x{ws}: max plane error {worst:.3g} of the window peak")
     assert worst < 0.05
+
+
+def test_precision_sweep_against_reference(cuda):
+    """Precision study on the reference's own c0 case (1024x1024, 32x32 windows) for the
+    three correlation paths: correlation-plane error against the FP64 oracle (sampled
+    windows), peak-index mismatch rate against the reference (all windows, and outside
+    near ties), and the main-peak displacement difference where the index agrees.  The
+    FP32 and split-BF16 paths hold the parity bar; single-product BF16 is reported."""
+    from test_gpu_golden import load, near_ties
+
+    z = load("c0")
+    sk = ast.literal_eval(str(z["synth"][0]))
+    pk = ast.literal_eval(str(z["params"][0]))
+    f1, f2 = P.synth_pair(P.synth_params(**sk))
+    p = P.default_params(**pk)
+    rows = []
+    for name, path in (("fp32 simt", P.PIV_XCORR_SIMT), ("split-bf16 tc", P.PIV_XCORR_TC_SPLIT),
+                       ("bf16 tc", P.PIV_XCORR_TC_BF16)):
+        with P.Engine(p) as e:
+            e.set_xcorr_path(0, path)
+            e.set_images(f1, f2)
+            e.prep()
+            e.pass_grid1(0)
+            nt = e.geom["Nt_vec"][0]
+            planes = e.cc_planes(0, 0, nt)
+            _, idx, _ = e.peaks(0)
+            _, _, dx, dy, v = e.field(0)
+            geom = e.geom
+        ws = p.ws_x1
+        w1 = _gather(f1, geom, 0, ws, p.spacing_x1)
+        w2 = _gather(f2, geom, 0, ws, p.spacing_x1)
+        perr = 0.0
+        for w in range(0, nt, max(1, nt // 40)):
+            want = O.xcorr_plane(w1[w], w2[w])
+            perr = max(perr, np.abs(planes[w] - want).max() / max(want.max(), 1.0))
+        ref_idx = z["peaks0_index"]
+        tie_top, _ = near_ties(planes, geom["border_x"][0], geom["border_y"][0], p.Npeak_save, rel=1e-4)
+        mism_all = np.mean(np.any(idx != ref_idx, axis=1))
+        mism_clean = np.mean(np.any(idx[~tie_top] != ref_idx[~tie_top], axis=1))
+        main = (idx[:, 0] == ref_idx[:, 0]) & (v[:, 0] == 1) & (z["raw0_valid"][:, 0] == 1)
+        d = np.maximum(np.abs(dx[:, 0] - z["raw0_dx"][:, 0]), np.abs(dy[:, 0] - z["raw0_dy"][:, 0]))[main]
+        rows.append((name, perr, mism_all, mism_clean, float(np.median(d)), float(np.percentile(d, 99.9)),
+                     float(d.max())))
+    print("\npath            plane err   idx mismatch (all / no near-ties)   |d| median   99.9%      max  [px]")
+    for r in rows:
+        print(f"{r[0]:15s} {r[1]:9.2e}   {r[2]:9.4%} / {r[3]:9.4%}          {r[4]:9.2e}  {r[5]:9.2e} {r[6]:9.2e}")
+    fp32, split, bf16 = rows
+    for r in (fp32, split):
+        assert r[1] <= PLANE_REL and r[3] == 0.0 and r[5] <= 1e-3
+    assert bf16[1] < 0.05
