@@ -366,8 +366,19 @@ __device__ __forceinline__ void peak_window_merge(const XcorrArgs &a, const floa
     peak_fit_store<WSX, WSY>(a, P, w, lane, v, idx, parts[0].cnt + parts[1].cnt, pred_x, pred_y);
 }
 
+// Residency asked of the register allocation (the second __launch_bounds__ argument).
+// 32x32 windows, 4 per CTA of 128 threads: 33.8 KB of shared memory lets 6 CTAs share an
+// SM, and at 80 registers (checked spill-free) so do the registers, against 5 CTAs at the
+// unconstrained 84.  Elsewhere the compiler's own choice (a blanket bound makes the small
+// variants spill).
+template <int WSX, int WSY, int B, int NT>
+constexpr int xcorr_min_ctas()
+{
+    return (WSX == 32 && WSY == 32 && B == 4 && NT == 128) ? 6 : 1;
+}
+
 template <int WSX, int WSY, int B, int NT, int K, bool DEF>
-__global__ void __launch_bounds__(NT) xcorr_peak_kernel(const XcorrArgs a)
+__global__ void __launch_bounds__(NT, (xcorr_min_ctas<WSX, WSY, B, NT>())) xcorr_peak_kernel(const XcorrArgs a)
 {
     static_assert(B % 2 == 0, "windows are processed in pairs");
     static_assert(NT % 32 == 0, "the peak stage works in whole warps");
