@@ -127,4 +127,42 @@ __device__ __forceinline__ void fft(float2 (&x)[N])
     }
 }
 
+// Two-thread transform of length N (N % 4 == 0) by a lane pair (lanes l and l ^ 1, both
+// in `mask`).  Decimation in time by 2: half 0 holds x[2j], half 1 holds x[2j + 1]
+// (j < N/2) in y, each transforms its half (E, O), and after an exchange of N/4 values
+// each finishes half of the radix-2 step  X[k] = E[k] + W^k O[k],  X[k + N/2] =
+// E[k] - W^k O[k], for k = half*N/4 + j, j < N/4  (W^(N/4 + j) = W^(N/4) W^j).
+// Output: y[m] = X[fft2t_index<N>(m, half)].
+template <int N>
+__device__ __forceinline__ int fft2t_index(int m, int half)
+{
+    return m < N / 4 ? half * (N / 4) + m : N / 2 + half * (N / 4) + (m - N / 4);
+}
+
+template <int N, bool INV>
+__device__ __forceinline__ void fft2t(float2 (&y)[N / 2], int half, unsigned mask)
+{
+    static_assert(N % 4 == 0, "two-thread transform of a length divisible by 4");
+    constexpr int Q = N / 4;
+    fft<N / 2, INV>(y);
+    // half 0 keeps E[0, Q) and needs O[0, Q); half 1 keeps O[Q, 2Q) and needs E[Q, 2Q)
+    float2 e[Q], o[Q];
+#pragma unroll
+    for (int j = 0; j < Q; ++j) {
+        const float2 send = half ? y[j] : y[j + Q];
+        float2 recv;
+        recv.x = __shfl_xor_sync(mask, send.x, 1);
+        recv.y = __shfl_xor_sync(mask, send.y, 1);
+        e[j] = half ? recv : y[j];
+        o[j] = half ? y[j + Q] : recv;
+    }
+    static_for<0, Q>([&](auto jc) {
+        constexpr int j = decltype(jc)::value;
+        const float2 t0 = twiddle<N, INV, j>(o[j]);
+        const float2 t = half ? rot_quarter<INV>(t0) : t0;
+        y[j] = cadd(e[j], t);
+        y[j + Q] = csub(e[j], t);
+    });
+}
+
 }  // namespace piv

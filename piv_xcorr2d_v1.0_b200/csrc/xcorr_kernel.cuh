@@ -18,11 +18,13 @@
 //   P1  row task (window, row): gather frame-1 and frame-2 rows straight from HBM,
 //       pack z = f1 + i*f2, row FFT in registers, store.
 //   P2  column task: column FFT in registers -> Z = FFT2(f1) + i*FFT2(f2).
-//   P3  column task (window pair, column): the cross spectrum conj(F1)*F2 follows
+//   P3  column task (window pair, column; a lane pair per task for long columns when
+//       the CTA has the threads): the cross spectrum conj(F1)*F2 follows
 //       from Z(k) and Z(-k) as  C = Im(Z(k)Z(-k))/2 + i(|Z(-k)|^2 - |Z(k)|^2)/4;
 //       it is Hermitian, so two windows share one inverse transform:
 //       W = C_a + i*C_b, inverse column FFT in registers.
-//   P4  row task (pair, row): inverse row FFT -> Re = corr_a, Im = corr_b;
+//   P4  row task (pair, row; a lane pair per task likewise): inverse row FFT ->
+//       Re = corr_a, Im = corr_b;
 //       |.|/N written as fftshifted FP32 planes.
 //   P5  warp per window (two warps for windows taller than 32 rows when the CTA has
 //       them): 4-neighbour local maxima inside the search region,
@@ -435,16 +437,24 @@ __global__ void __launch_bounds__(NT, (xcorr_min_ctas<WSX, WSY, B, NT>())) xcorr
     __syncthreads();
 
     // ---------------- P3: cross spectrum of a window pair + inverse column FFT ----------------
+    // A pair task has one column per window pair, so half of the CTA would idle: for long
+    // columns (48 and more; measured: it loses at 32) and where the CTA has the threads, a
+    // lane pair shares each column (rows split by parity, fft2t).
+    constexpr bool P3_PAIRED = 2 * (B / 2) * WSX <= NT && WSY % 4 == 0 && WSY >= 48;
     static_assert((B / 2) * WSX <= NT, "one P3 task per thread");
     {
-        const bool active = tid < (B / 2) * WSX;
-        const int q = active ? tid / WSX : 0, c = active ? tid - (tid / WSX) * WSX : 0;
+        constexpr int NR = P3_PAIRED ? WSY / 2 : WSY;  // rows per thread
+        const int task = P3_PAIRED ? tid >> 1 : tid, half = P3_PAIRED ? tid & 1 : 0;
+        const bool active = task < (B / 2) * WSX;
+        const unsigned mask = __ballot_sync(0xffffffffu, active);
+        const int q = active ? task / WSX : 0, c = active ? task - (task / WSX) * WSX : 0;
         const int cm = (WSX - c) % WSX;
-        float2 wv[WSY];
+        float2 wv[NR];
         if (active) {
             const float2 *za = sm + (2 * q) * WIN, *zb = sm + (2 * q + 1) * WIN;
 #pragma unroll
-            for (int r = 0; r < WSY; ++r) {
+            for (int jj = 0; jj < NR; ++jj) {
+                const int r = P3_PAIRED ? 2 * jj + half : jj;
                 const int rm = (WSY - r) % WSY;
                 float2 A = za[r * LDX + c], M = za[rm * LDX + cm];
                 // C = Im(A*M)/2 + i*(|M|^2 - |A|^2)/4
@@ -454,35 +464,65 @@ __global__ void __launch_bounds__(NT, (xcorr_min_ctas<WSX, WSY, B, NT>())) xcorr
                 M = zb[rm * LDX + cm];
                 float2 Cb = make_float2(0.5f * (A.x * M.y + A.y * M.x),
                                         0.25f * ((M.x * M.x + M.y * M.y) - (A.x * A.x + A.y * A.y)));
-                wv[r] = make_float2(Ca.x - Cb.y, Ca.y + Cb.x);  // C_a + i*C_b
+                wv[jj] = make_float2(Ca.x - Cb.y, Ca.y + Cb.x);  // C_a + i*C_b
             }
-            fft<WSY, true>(wv);
+            if constexpr (P3_PAIRED) fft2t<WSY, true>(wv, half, mask);
+            else fft<WSY, true>(wv);
         }
         __syncthreads();  // every partner-column read is done
         if (active) {
             float2 *col = sm + (2 * q) * WIN + c;
 #pragma unroll
-            for (int r = 0; r < WSY; ++r) col[r * LDX] = wv[r];
+            for (int m = 0; m < NR; ++m) {
+                const int r = P3_PAIRED ? fft2t_index<WSY>(m, half) : m;
+                col[r * LDX] = wv[m];
+            }
         }
     }
     __syncthreads();
 
     // ---------------- P4: inverse row FFT -> two shifted FP32 planes ----------------
-    for (int t = tid; t < (B / 2) * WSY; t += NT) {
-        const int q = t / WSY, r = t - q * WSY;
-        const float2 *row = sm + (2 * q) * WIN + r * LDX;
-        float2 z[WSX];
+    // lane pairs per row for long rows (48 and more) where the CTA has the threads
+    // (columns split by parity, fft2t)
+    constexpr bool P4_PAIRED = 2 * (B / 2) * WSY <= NT && WSX % 4 == 0 && WSX >= 48;
+    if constexpr (P4_PAIRED) {
+        const int task = tid >> 1, half = tid & 1;
+        const bool active = task < (B / 2) * WSY;
+        const unsigned mask = __ballot_sync(0xffffffffu, active);
+        if (active) {
+            const int q = task / WSY, r = task - q * WSY;
+            const float2 *row = sm + (2 * q) * WIN + r * LDX;
+            float2 z[WSX / 2];
 #pragma unroll
-        for (int i = 0; i < WSX; ++i) z[i] = row[i];
-        fft<WSX, true>(z);
-        float *pa = reinterpret_cast<float *>(sm + (2 * q + 1) * WIN);
-        float *pb = pa + WSY * LDF;
-        const int rs = (r + WSY / 2) % WSY;
+            for (int jj = 0; jj < WSX / 2; ++jj) z[jj] = row[2 * jj + half];
+            fft2t<WSX, true>(z, half, mask);
+            float *pa = reinterpret_cast<float *>(sm + (2 * q + 1) * WIN);
+            float *pb = pa + WSY * LDF;
+            const int rs = (r + WSY / 2) % WSY;
 #pragma unroll
-        for (int i = 0; i < WSX; ++i) {
-            const int is = (i + WSX / 2) % WSX;
-            pa[rs * LDF + is] = fabsf(z[i].x) * inv_n;
-            pb[rs * LDF + is] = fabsf(z[i].y) * inv_n;
+            for (int m = 0; m < WSX / 2; ++m) {
+                const int is = (fft2t_index<WSX>(m, half) + WSX / 2) % WSX;
+                pa[rs * LDF + is] = fabsf(z[m].x) * inv_n;
+                pb[rs * LDF + is] = fabsf(z[m].y) * inv_n;
+            }
+        }
+    } else {
+        for (int t = tid; t < (B / 2) * WSY; t += NT) {
+            const int q = t / WSY, r = t - q * WSY;
+            const float2 *row = sm + (2 * q) * WIN + r * LDX;
+            float2 z[WSX];
+#pragma unroll
+            for (int i = 0; i < WSX; ++i) z[i] = row[i];
+            fft<WSX, true>(z);
+            float *pa = reinterpret_cast<float *>(sm + (2 * q + 1) * WIN);
+            float *pb = pa + WSY * LDF;
+            const int rs = (r + WSY / 2) % WSY;
+#pragma unroll
+            for (int i = 0; i < WSX; ++i) {
+                const int is = (i + WSX / 2) % WSX;
+                pa[rs * LDF + is] = fabsf(z[i].x) * inv_n;
+                pb[rs * LDF + is] = fabsf(z[i].y) * inv_n;
+            }
         }
     }
     __syncthreads();
