@@ -403,13 +403,15 @@ __global__ void __launch_bounds__(128) median_pass_kernel(const MedianPass a)
                 bitonic_sort<32>(xs);
                 bitonic_sort<32>(ys);
                 const float mx = median_sorted<32>(xs, n), my = median_sorted<32>(ys, n);
+                // |x - median| over a sorted x falls, then rises (then +inf): a bitonic
+                // sequence, which the final merge stage of the network sorts on its own
 #pragma unroll
                 for (int q = 0; q < 32; ++q) {
                     xs[q] = (q < n) ? fabsf(xs[q] - mx) : inf;
                     ys[q] = (q < n) ? fabsf(ys[q] - my) : inf;
                 }
-                bitonic_sort<32>(xs);
-                bitonic_sort<32>(ys);
+                bitonic_step<32, 32, 16>(xs);
+                bitonic_step<32, 32, 16>(ys);
                 const float dmx = median_sorted<32>(xs, n), dmy = median_sorted<32>(ys, n);
                 median_decide(a, v, mx, my, dmx, dmy, rx, ry, rv);
             }
