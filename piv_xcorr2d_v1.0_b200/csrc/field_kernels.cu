@@ -386,9 +386,9 @@ __global__ void __launch_bounds__(128) median_pass_kernel(const MedianPass a)
             const float inf = __int_as_float(0x7f800000);
             float xs[32], ys[32];
             int n = 0;
+            int tx = 0, ty = 0;  // stencil column and row of slot t (no division per slot)
 #pragma unroll
             for (int t = 0; t < 32; ++t) {
-                const int ty = t / a.wx, tx = t - ty * a.wx;
                 const int x = vx - hfwx + tx, y = vy - hfwy + ty;
                 const bool inb = (t < Ntm) & (t != centre) & (x >= 0) & (x <= a.Nx - 1) & (y >= 0) & (y <= a.Ny - 1);
                 bool ok;
@@ -398,6 +398,9 @@ __global__ void __launch_bounds__(128) median_pass_kernel(const MedianPass a)
                 xs[t] = ok ? px : inf;
                 ys[t] = ok ? py : inf;
                 n += ok;
+                const bool wrap = ++tx == a.wx;
+                tx = wrap ? 0 : tx;
+                ty += wrap;
             }
             if (n >= a.minN && n >= 1) {
                 bitonic_sort<32>(xs);
