@@ -127,8 +127,9 @@ __device__ __forceinline__ void fft(float2 (&x)[N])
     }
 }
 
-// Two-thread transform of length N (N % 4 == 0) by a lane pair (lanes l and l ^ 1, both
-// in `mask`).  Decimation in time by 2: half 0 holds x[2j], half 1 holds x[2j + 1]
+// Two-thread transform of length N (N % 4 == 0) by a lane pair (lanes l and l ^ 16, both
+// in `mask`; the halves sit in different half-warps, so the pair's 8-byte shared-memory
+// accesses do not share banks).  Decimation in time by 2: half 0 holds x[2j], half 1 holds x[2j + 1]
 // (j < N/2) in y, each transforms its half (E, O), and after an exchange of N/4 values
 // each finishes half of the radix-2 step  X[k] = E[k] + W^k O[k],  X[k + N/2] =
 // E[k] - W^k O[k], for k = half*N/4 + j, j < N/4  (W^(N/4 + j) = W^(N/4) W^j).
@@ -151,8 +152,8 @@ __device__ __forceinline__ void fft2t(float2 (&y)[N / 2], int half, unsigned mas
     for (int j = 0; j < Q; ++j) {
         const float2 send = half ? y[j] : y[j + Q];
         float2 recv;
-        recv.x = __shfl_xor_sync(mask, send.x, 1);
-        recv.y = __shfl_xor_sync(mask, send.y, 1);
+        recv.x = __shfl_xor_sync(mask, send.x, 16);
+        recv.y = __shfl_xor_sync(mask, send.y, 16);
         e[j] = half ? recv : y[j];
         o[j] = half ? y[j + Q] : recv;
     }

@@ -18,8 +18,8 @@
 //   P1  row task (window, row): gather frame-1 and frame-2 rows straight from HBM,
 //       pack z = f1 + i*f2, row FFT in registers, store.
 //   P2  column task: column FFT in registers -> Z = FFT2(f1) + i*FFT2(f2).
-//   P3  column task (window pair, column; a lane pair per task for long columns when
-//       the CTA has the threads): the cross spectrum conj(F1)*F2 follows
+//   P3  column task (window pair, column; a lane pair per task for columns of 32 and
+//       more when the CTA has the threads): the cross spectrum conj(F1)*F2 follows
 //       from Z(k) and Z(-k) as  C = Im(Z(k)Z(-k))/2 + i(|Z(-k)|^2 - |Z(k)|^2)/4;
 //       it is Hermitian, so two windows share one inverse transform:
 //       W = C_a + i*C_b, inverse column FFT in registers.
@@ -437,14 +437,15 @@ __global__ void __launch_bounds__(NT, (xcorr_min_ctas<WSX, WSY, B, NT>())) xcorr
     __syncthreads();
 
     // ---------------- P3: cross spectrum of a window pair + inverse column FFT ----------------
-    // A pair task has one column per window pair, so half of the CTA would idle: for long
-    // columns (48 and more; measured: it loses at 32) and where the CTA has the threads, a
-    // lane pair shares each column (rows split by parity, fft2t).
-    constexpr bool P3_PAIRED = 2 * (B / 2) * WSX <= NT && WSY % 4 == 0 && WSY >= 48;
+    // A pair task has one column per window pair, so half of the CTA would idle: for
+    // columns of 32 and more (measured gains at 32 and 64) and where the CTA has the
+    // threads, a lane pair shares each column (rows split by parity, fft2t).
+    constexpr bool P3_PAIRED = 2 * (B / 2) * WSX <= NT && WSY % 4 == 0 && WSY >= 32;
     static_assert((B / 2) * WSX <= NT, "one P3 task per thread");
     {
         constexpr int NR = P3_PAIRED ? WSY / 2 : WSY;  // rows per thread
-        const int task = P3_PAIRED ? tid >> 1 : tid, half = P3_PAIRED ? tid & 1 : 0;
+        // pair: lanes l and l + 16 of a warp (16 tasks per warp)
+        const int task = P3_PAIRED ? (tid >> 5) * 16 + (tid & 15) : tid, half = P3_PAIRED ? (tid >> 4) & 1 : 0;
         const bool active = task < (B / 2) * WSX;
         const unsigned mask = __ballot_sync(0xffffffffu, active);
         const int q = active ? task / WSX : 0, c = active ? task - (task / WSX) * WSX : 0;
@@ -482,11 +483,11 @@ __global__ void __launch_bounds__(NT, (xcorr_min_ctas<WSX, WSY, B, NT>())) xcorr
     __syncthreads();
 
     // ---------------- P4: inverse row FFT -> two shifted FP32 planes ----------------
-    // lane pairs per row for long rows (48 and more) where the CTA has the threads
-    // (columns split by parity, fft2t)
-    constexpr bool P4_PAIRED = 2 * (B / 2) * WSY <= NT && WSX % 4 == 0 && WSX >= 48;
+    // lane pairs per row for rows of 32 and more where the CTA has the threads (columns
+    // split by parity, fft2t)
+    constexpr bool P4_PAIRED = 2 * (B / 2) * WSY <= NT && WSX % 4 == 0 && WSX >= 32;
     if constexpr (P4_PAIRED) {
-        const int task = tid >> 1, half = tid & 1;
+        const int task = (tid >> 5) * 16 + (tid & 15), half = (tid >> 4) & 1;  // lanes l, l + 16
         const bool active = task < (B / 2) * WSY;
         const unsigned mask = __ballot_sync(0xffffffffu, active);
         if (active) {
