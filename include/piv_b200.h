@@ -196,6 +196,18 @@ int piv_synchronize(piv_engine *e);
  * Any output pointer may be NULL. */
 int piv_get_field(piv_engine *e, int selection, float *x, float *y, float *dx, float *dy, uint8_t *valid);
 
+/* Asynchronous readback (no counterpart in the reference, which reads each field back
+ * before the next pair starts).  piv_field_async queues, behind the work already queued on
+ * the engine stream, the copy of a selection (0..3, as piv_get_field) into one of two
+ * engine-owned pinned slots, together with the device status word of that work, and
+ * returns at once with a ticket.  piv_field_wait waits for that copy, reports a device
+ * error of its pair (PIV_ERR_DEVICE), and copies the arrays out (any pointer may be NULL).
+ * A caller thus keeps the next pair queued while it reads the previous one:
+ *   queue(0); for k: run(k); t[k] = field_async(k); queue(k+1); field_wait(t[k-1]).
+ * At most two readbacks are pending (PIV_ERR_STATE otherwise). */
+int piv_field_async(piv_engine *e, int selection, int *ticket);
+int piv_field_wait(piv_engine *e, int ticket, float *x, float *y, float *dx, float *dy, uint8_t *valid);
+
 /* write_vec_data_general (X/xcorr2d_multi_grid.cu:1865-1973): Tecplot ASCII file. */
 int piv_write_tecplot(piv_engine *e, const char *path, int selection);
 

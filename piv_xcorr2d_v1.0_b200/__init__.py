@@ -141,6 +141,8 @@ EXPORTS = {
     "piv_time_stage": (C.c_int, [_P, C.c_int, C.c_int, _F]),
     "piv_probe_fp32_peak": (C.c_int, [_F]),
     "piv_queue_images": (C.c_int, [_P, _P, _P]),
+    "piv_field_async": (C.c_int, [_P, C.c_int, C.POINTER(C.c_int)]),
+    "piv_field_wait": (C.c_int, [_P, C.c_int, _F, _F, _F, _F, _U8]),
     "piv_host_alloc": (C.c_int, [C.c_size_t, C.POINTER(_P)]),
     "piv_host_free": (C.c_int, [_P]),
     "piv_set_xcorr_path": (C.c_int, [_P, C.c_int, C.c_int]),
@@ -388,6 +390,30 @@ class Engine:
             dx = dx.reshape(nt, -1)
             dy = dy.reshape(nt, -1)
             v = v.reshape(nt, -1)
+        return x, y, dx, dy, v
+
+    def field_async(self, selection):
+        """Queues the readback of a selection behind the queued work; returns a ticket."""
+        t = C.c_int(0)
+        self._ck(lib().piv_field_async(self.h, selection, C.byref(t)))
+        return (t.value, selection)
+
+    def field_wait(self, ticket):
+        """(x, y, dx, dy, valid) of a piv_field_async ticket, as field() returns them."""
+        t, selection = ticket
+        g = 0 if selection < 2 else 1
+        nt = self._nt(g)
+        raw = selection in (0, 2)
+        n = nt * self.p.Npeak_save if raw else nt
+        x = np.empty(nt, np.float32)
+        y = np.empty(nt, np.float32)
+        dx = np.empty(n, np.float32)
+        dy = np.empty(n, np.float32)
+        v = np.empty(n, np.uint8)
+        self._ck(lib().piv_field_wait(self.h, t, _ptr(x, C.c_float), _ptr(y, C.c_float), _ptr(dx, C.c_float),
+                                      _ptr(dy, C.c_float), _ptr(v, C.c_uint8)))
+        if raw:
+            dx, dy, v = dx.reshape(nt, -1), dy.reshape(nt, -1), v.reshape(nt, -1)
         return x, y, dx, dy, v
 
     def peaks(self, grid):

@@ -157,6 +157,18 @@ struct piv_engine {
     cudaEvent_t ev_up[2] = {}, ev_done[2] = {};
     bool slot_read[2] = {};
     int next_slot = 0, pending_slot = -1, reading_slot = -1;
+    // asynchronous readback (piv_field_async / piv_field_wait): two pinned result slots
+    struct ResultSlot {
+        float *dx = nullptr, *dy = nullptr;
+        uint8_t *valid = nullptr;
+        int *status = nullptr;
+        size_t cap = 0;       // elements the slot holds
+        int sel = 0, seq = 0;
+        bool pending = false;
+        cudaEvent_t ev = nullptr;
+    };
+    ResultSlot results[2];
+    int result_seq = 0;
     std::string err;
     bool timing = false;
     cudaEvent_t ev[6] = {};
@@ -214,6 +226,13 @@ void free_all(piv_engine *e)
         if (e->ev_done[q]) cudaEventDestroy(e->ev_done[q]);
     }
     if (e->copy_stream) cudaStreamDestroy(e->copy_stream);
+    for (auto &r : e->results) {
+        cudaFreeHost(r.dx);
+        cudaFreeHost(r.dy);
+        cudaFreeHost(r.valid);
+        cudaFreeHost(r.status);
+        if (r.ev) cudaEventDestroy(r.ev);
+    }
     cudaFreeHost(e->h_f1);
     cudaFreeHost(e->h_f2);
     cudaFreeHost(e->h_status);
@@ -998,6 +1017,78 @@ int piv_get_field(piv_engine *e, int sel, float *x, float *y, float *dx, float *
             }
     }
     CK(cudaStreamSynchronize(e->stream));
+    return PIV_OK;
+}
+
+int piv_field_async(piv_engine *e, int sel, int *ticket)
+{
+    int rc = check_ready(e, false);
+    if (rc) return rc;
+    if (sel < 0 || sel > 3 || !ticket) return set_err(e, PIV_ERR_ARG, "selection must be 0..3 and ticket non-NULL");
+    int q = -1;
+    for (int i = 0; i < 2 && q < 0; ++i)
+        if (!e->results[i].pending) q = i;
+    if (q < 0) return set_err(e, PIV_ERR_STATE, "two readbacks are pending: wait for one first");
+    piv_engine::ResultSlot &r = e->results[q];
+    const int k = sel / 2;
+    const bool raw = (sel % 2) == 0;
+    const GridState &gs = e->grid[k];
+    const size_t Nt = (size_t)gs.gg.Nt_vec, n = raw ? Nt * e->p.Npeak_save : Nt;
+    if (r.cap < n) {
+        cudaFreeHost(r.dx);
+        cudaFreeHost(r.dy);
+        cudaFreeHost(r.valid);
+        r.dx = r.dy = nullptr;
+        r.valid = nullptr;
+        r.cap = 0;
+        if (cudaHostAlloc((void **)&r.dx, n * sizeof(float), cudaHostAllocDefault) != cudaSuccess ||
+            cudaHostAlloc((void **)&r.dy, n * sizeof(float), cudaHostAllocDefault) != cudaSuccess ||
+            cudaHostAlloc((void **)&r.valid, n, cudaHostAllocDefault) != cudaSuccess)
+            return set_err(e, PIV_ERR_ALLOC, "cudaMallocHost ERROR! (readback slot)");
+        r.cap = n;
+    }
+    if (!r.status && cudaHostAlloc((void **)&r.status, sizeof(int), cudaHostAllocDefault) != cudaSuccess)
+        return set_err(e, PIV_ERR_ALLOC, "cudaMallocHost ERROR! (readback status)");
+    if (!r.ev) CK(cudaEventCreateWithFlags(&r.ev, cudaEventDisableTiming));
+    CK(cudaMemcpyAsync(r.dx, raw ? gs.cdx : gs.fx, n * sizeof(float), cudaMemcpyDeviceToHost, e->stream));
+    CK(cudaMemcpyAsync(r.dy, raw ? gs.cdy : gs.fy, n * sizeof(float), cudaMemcpyDeviceToHost, e->stream));
+    CK(cudaMemcpyAsync(r.valid, raw ? gs.cv : gs.fv, n, cudaMemcpyDeviceToHost, e->stream));
+    // the status word of the work behind this readback travels with it, then restarts at 0
+    CK(cudaMemcpyAsync(r.status, e->d_status, sizeof(int), cudaMemcpyDeviceToHost, e->stream));
+    CK(cudaMemsetAsync(e->d_status, 0, sizeof(int), e->stream));
+    CK(cudaEventRecord(r.ev, e->stream));
+    r.sel = sel;
+    r.seq = ++e->result_seq;
+    r.pending = true;
+    *ticket = q | (r.seq << 1);
+    return PIV_OK;
+}
+
+int piv_field_wait(piv_engine *e, int ticket, float *x, float *y, float *dx, float *dy, uint8_t *valid)
+{
+    if (!e || ticket < 2) return PIV_ERR_ARG;
+    piv_engine::ResultSlot &r = e->results[ticket & 1];
+    if (!r.pending || r.seq != (ticket >> 1)) return set_err(e, PIV_ERR_STATE, "no pending readback with this ticket");
+    cudaSetDevice(e->device);
+    CK(cudaEventSynchronize(r.ev));
+    r.pending = false;
+    if (*r.status)
+        return set_err(e, PIV_ERR_DEVICE, "device status 0x%x (%s)", *r.status,
+                       (*r.status & kStatusMmaWait) ? "tensor-core MMA completion wait timed out"
+                                                    : "hole-fill iteration cap reached");
+    const GridState &gs = e->grid[r.sel / 2];
+    const size_t Nt = (size_t)gs.gg.Nt_vec, n = (r.sel % 2 == 0) ? Nt * e->p.Npeak_save : Nt;
+    if (dx) std::memcpy(dx, r.dx, n * sizeof(float));
+    if (dy) std::memcpy(dy, r.dy, n * sizeof(float));
+    if (valid) std::memcpy(valid, r.valid, n);
+    if (x || y) {
+        for (int j = 0; j < gs.gg.Ny_vec; ++j)
+            for (int i = 0; i < gs.gg.Nx_vec; ++i) {
+                // grid coordinates of X/xcorr2d_multi_grid.cu:1237-1254
+                if (x) x[j * gs.gg.Nx_vec + i] = (float)(gs.gg.sp_x / 2 + i * gs.gg.sp_x);
+                if (y) y[j * gs.gg.Nx_vec + i] = (float)(gs.gg.sp_y / 2 + j * gs.gg.sp_y);
+            }
+    }
     return PIV_OK;
 }
 

@@ -70,3 +70,51 @@ def test_queue_twice_is_refused_and_set_images_discards(cuda):
         again = e.field(3)
         for a, b in zip(got, again):
             assert np.array_equal(a, b)
+
+
+def test_async_readback_pipeline(cuda):
+    """Queued uploads and asynchronous readbacks together: every pair's field matches the
+    one-at-a-time path bit for bit although the next pair is always queued, and its
+    readback enqueued, before the previous pair's results are collected; at most two
+    readbacks may be pending, and a stale ticket is refused."""
+    import torch
+
+    Nx, Ny = 480, 400
+    pairs = _pairs(4, Nx, Ny)
+    p = _params(Nx, Ny, 1)
+    want = []
+    with P.Engine(p) as e:
+        for f1, f2 in pairs:
+            e.set_images(f1, f2)
+            e.run_pair()
+            want.append((e.field(3), e.field(2)))
+    pinned = [(torch.from_numpy(f1).pin_memory(), torch.from_numpy(f2).pin_memory()) for f1, f2 in pairs]
+    with P.Engine(p) as e:
+        got = []
+        e.queue_images(*pinned[0])
+        prev = None
+        for k in range(len(pairs)):
+            e.run_pair()
+            tk = e.field_async(3)
+            if k + 1 < len(pairs):
+                e.queue_images(*pinned[k + 1])
+            if prev is not None:
+                got.append(e.field_wait(prev))
+            prev = tk
+        got.append(e.field_wait(prev))
+        with pytest.raises(P.PivError):
+            e.field_wait(prev)  # already collected
+        # both slots in use: a third pending readback is refused until one is collected
+        ta, tb = e.field_async(3), e.field_async(2)
+        with pytest.raises(P.PivError) as ex:
+            e.field_async(0)
+        assert ex.value.status == P.PIV_ERR_STATE
+        raw2 = e.field_wait(tb)
+        last3 = e.field_wait(ta)
+    for k in range(len(pairs)):
+        for a, b in zip(got[k], want[k][0]):
+            assert np.array_equal(a, b), f"pair {k}"
+    for a, b in zip(last3, want[-1][0]):
+        assert np.array_equal(a, b)
+    for a, b in zip(raw2, want[-1][1]):
+        assert np.array_equal(a, b)
