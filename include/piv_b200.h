@@ -356,6 +356,63 @@ int piv_synth_pair(const piv_synth_params *s, uint8_t *f1, uint8_t *f2);
 /* The displacement field of s evaluated at n points. */
 int piv_synth_field(const piv_synth_params *s, const float *x, const float *y, int n, float *u, float *v);
 
+/* The same pair rendered on the GPU from the same random streams (particles, field,
+ * noise); the float accumulation order differs, so a pixel may differ from the host
+ * generator by one grey level at a rounding tie.  d_f1, d_f2: Nx*Ny bytes each (device);
+ * d_scratch: 2*Nx*Ny floats (device); stream: cudaStream_t or NULL.  Asynchronous. */
+int piv_synth_pair_device(const piv_synth_params *s, uint8_t *d_f1, uint8_t *d_f2, float *d_scratch, void *stream);
+
+/* ---- learned grid-1 predictor (no reference counterpart) --------------------------
+ * Replaces the plain grid-1 passes (X/main.cpp:290-300 driving Calc_cc_map_p1 and
+ * MedianFilter_Smoothing_p1) as the deformation predictor of the grid-2 passes.
+ *   features: both frames box-averaged 4x4 (grey/255, global mean removed); at every
+ *     grid-1 vector a (ws_x1/4 x ws_y1/4) window of frame 1 correlated with frame 2 at
+ *     the 81 integer shifts |dx|,|dy| <= 4 of the downsampled grid, normalised by the
+ *     windows' energies -> input [81][Ny1_vec][Nx1_vec];
+ *   network: 4-level U-Net on the grid-1 vector grid (3x3 convolutions, LeakyReLU 0.1,
+ *     stride-2 down, nearest-up + skip concatenation, 881,922 parameters), BF16 weights,
+ *     FP32 activations and accumulation; output [2][Ny1_vec][Nx1_vec] in downsampled
+ *     pixels (x4 = image pixels).
+ * Training (piv_net_loss_grad + piv_net_adam_step) and inference run on hand-written
+ * kernels; the net is bound to the device current at piv_net_create. */
+typedef struct piv_net piv_net;
+#define PIV_NET_IN_CHANNELS 81
+#define PIV_NET_LAYERS 13
+int piv_net_create(uint64_t seed, piv_net **out);
+int piv_net_destroy(piv_net *n);
+const char *piv_net_last_error(const piv_net *n);
+int piv_net_num_params(const piv_net *n, int64_t *count);
+/* Layer `layer` (0..12): input/output channels, stride, offsets of its weights
+ * [cout][cin][3][3] and biases [cout] in the flat parameter vector. */
+int piv_net_layout(int layer, int *cin, int *cout, int *stride, int *weight_offset, int *bias_offset);
+int piv_net_get_params(piv_net *n, float *host, int64_t count);
+int piv_net_set_params(piv_net *n, const float *host, int64_t count);  /* resets Adam */
+int piv_net_get_grads(piv_net *n, float *host, int64_t count);
+int piv_net_save(piv_net *n, const char *path);
+int piv_net_load(piv_net *n, const char *path);
+/* [N][81][H][W] -> [N][2][H][W] (device pointers); stream NULL = the net's own. */
+int piv_net_forward(piv_net *n, const float *d_in, int N, int H, int W, float *d_out, void *stream);
+/* Forward, Charbonnier loss against d_label [N][2][H][W] (downsampled px) over the
+ * vectors with d_mask [N][H][W] = 1 (mean over them), backward into the net's gradient
+ * buffer (overwritten).  Synchronous; *loss receives the loss. */
+int piv_net_loss_grad(piv_net *n, const float *d_in, const float *d_label, const float *d_mask, int N, int H, int W,
+                      float *loss);
+int piv_net_adam_step(piv_net *n, float lr);  /* Adam, beta 0.9/0.999, eps 1e-8 */
+int piv_net_synchronize(piv_net *n);
+
+/* The predictor input of the engine's current (prepared) frames at grid 1, written to
+ * d_out [81][Ny1_vec][Nx1_vec] on the engine's stream (asynchronous). */
+int piv_net_features(piv_engine *e, piv_net *n, float *d_out);
+/* The learned form of a pair: prep, features, network -> grid-1 field (all valid),
+ * upsampling, the Npass2 grid-2 passes with their validation (the grid's correlation
+ * path, piv_set_xcorr_path), then the judge: the fraction of grid-2 vectors the last
+ * median test rejected and the RMS difference between the upsampled prediction and the
+ * final grid-2 field.  Above max_reject_frac or max_rms_px, the pair is run again by the
+ * plain method (piv_run_pair) and *fell_back = 1.  Synchronous (the judge is read on the
+ * host).  Requires Npass2 > 0. */
+int piv_run_pair_learned(piv_engine *e, piv_net *n, float max_reject_frac, float max_rms_px, int *fell_back,
+                         float *reject_frac, float *rms_px);
+
 #ifdef __cplusplus
 }
 #endif

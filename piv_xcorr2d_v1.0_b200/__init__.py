@@ -154,6 +154,24 @@ EXPORTS = {
     "piv_mhe_process_noalloc": (C.c_int, [_P, _P, C.c_int, C.c_int, C.c_int, C.c_float, _P]),
     "piv_synth_pair": (C.c_int, [C.POINTER(PivSynthParams), _U8, _U8]),
     "piv_synth_field": (C.c_int, [C.POINTER(PivSynthParams), _F, _F, C.c_int, _F, _F]),
+    "piv_synth_pair_device": (C.c_int, [C.POINTER(PivSynthParams), _P, _P, _P, _P]),
+    "piv_net_create": (C.c_int, [C.c_uint64, C.POINTER(_P)]),
+    "piv_net_destroy": (C.c_int, [_P]),
+    "piv_net_last_error": (C.c_char_p, [_P]),
+    "piv_net_num_params": (C.c_int, [_P, C.POINTER(C.c_int64)]),
+    "piv_net_layout": (C.c_int, [C.c_int] + [C.POINTER(C.c_int)] * 5),
+    "piv_net_get_params": (C.c_int, [_P, _F, C.c_int64]),
+    "piv_net_set_params": (C.c_int, [_P, _F, C.c_int64]),
+    "piv_net_get_grads": (C.c_int, [_P, _F, C.c_int64]),
+    "piv_net_save": (C.c_int, [_P, C.c_char_p]),
+    "piv_net_load": (C.c_int, [_P, C.c_char_p]),
+    "piv_net_forward": (C.c_int, [_P, _P, C.c_int, C.c_int, C.c_int, _P, _P]),
+    "piv_net_loss_grad": (C.c_int, [_P, _P, _P, _P, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_float)]),
+    "piv_net_adam_step": (C.c_int, [_P, C.c_float]),
+    "piv_net_synchronize": (C.c_int, [_P]),
+    "piv_net_features": (C.c_int, [_P, _P, _P]),
+    "piv_run_pair_learned": (C.c_int, [_P, _P, C.c_float, C.c_float, C.POINTER(C.c_int), C.POINTER(C.c_float),
+                                        C.POINTER(C.c_float)]),
 }
 
 _lib_handle = None
@@ -271,6 +289,110 @@ def synth_field(s: PivSynthParams, x, y):
     if rc != PIV_OK:
         raise PivError(rc, "field evaluation failed")
     return u, v
+
+
+def _dptr(x) -> int:
+    """Device address of a torch tensor, or an int address as is."""
+    return x if isinstance(x, int) else int(x.data_ptr())
+
+
+def synth_pair_device(s: PivSynthParams, d_f1, d_f2, d_scratch, stream=None):
+    """The same pair as synth_pair rendered on the GPU (asynchronous on `stream`): d_f1, d_f2
+    hold Nx*Ny bytes, d_scratch 2*Nx*Ny floats (torch tensors or device addresses)."""
+    rc = lib().piv_synth_pair_device(C.byref(s), _dptr(d_f1), _dptr(d_f2), _dptr(d_scratch), stream)
+    if rc != PIV_OK:
+        raise PivError(rc, "device synthetic pair generation failed")
+
+
+NET_IN_CHANNELS = 81
+NET_LAYERS = 13
+
+
+def net_layout():
+    """[(cin, cout, stride, weight_offset, bias_offset)] of the predictor's 13 layers."""
+    out = []
+    for i in range(NET_LAYERS):
+        v = [C.c_int() for _ in range(5)]
+        rc = lib().piv_net_layout(i, *[C.byref(x) for x in v])
+        if rc != PIV_OK:
+            raise PivError(rc, "layout")
+        out.append(tuple(x.value for x in v))
+    return out
+
+
+class PredictorNet:
+    """The learned grid-1 predictor (piv_net_*): a 4-level U-Net on the cost volume of the
+    4x-downsampled frames, BF16 weights, hand-written training and inference kernels."""
+
+    def __init__(self, seed=1, weights=None):
+        h = C.c_void_p()
+        rc = lib().piv_net_create(seed, C.byref(h))
+        if rc != PIV_OK:
+            raise PivError(rc, "piv_net_create failed")
+        self.h = h
+        n = C.c_int64()
+        self._ck(lib().piv_net_num_params(self.h, C.byref(n)))
+        self.n_params = n.value
+        if weights is not None:
+            self.load(weights)
+
+    def _ck(self, rc):
+        if rc != PIV_OK:
+            raise PivError(rc, lib().piv_net_last_error(self.h).decode())
+        return rc
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().piv_net_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def params(self) -> np.ndarray:
+        out = np.empty(self.n_params, np.float32)
+        self._ck(lib().piv_net_get_params(self.h, _ptr(out, C.c_float), self.n_params))
+        return out
+
+    def set_params(self, v):
+        v = np.ascontiguousarray(v, np.float32)
+        self._ck(lib().piv_net_set_params(self.h, _ptr(v, C.c_float), v.size))
+
+    def grads(self) -> np.ndarray:
+        out = np.empty(self.n_params, np.float32)
+        self._ck(lib().piv_net_get_grads(self.h, _ptr(out, C.c_float), self.n_params))
+        return out
+
+    def save(self, path):
+        self._ck(lib().piv_net_save(self.h, str(path).encode()))
+
+    def load(self, path):
+        self._ck(lib().piv_net_load(self.h, str(path).encode()))
+
+    def forward(self, d_in, N, H, W, d_out, stream=None):
+        """[N][81][H][W] -> [N][2][H][W] (downsampled px), device buffers."""
+        self._ck(lib().piv_net_forward(self.h, _dptr(d_in), N, H, W, _dptr(d_out), stream))
+
+    def loss_grad(self, d_in, d_label, d_mask, N, H, W) -> float:
+        loss = C.c_float()
+        self._ck(lib().piv_net_loss_grad(self.h, _dptr(d_in), _dptr(d_label), _dptr(d_mask), N, H, W,
+                                         C.byref(loss)))
+        return loss.value
+
+    def adam_step(self, lr):
+        self._ck(lib().piv_net_adam_step(self.h, lr))
+
+    def synchronize(self):
+        self._ck(lib().piv_net_synchronize(self.h))
 
 
 class Engine:
@@ -464,6 +586,18 @@ class Engine:
         out = np.zeros(5, np.float32)
         self._ck(lib().piv_stage_times(self.h, _ptr(out, C.c_float)))
         return out
+
+    # -- learned form --
+    def features(self, net: PredictorNet, d_out):
+        """The predictor input of the prepared frames, [81][Ny1_vec][Nx1_vec] into d_out."""
+        self._ck(lib().piv_net_features(self.h, net.h, _dptr(d_out)))
+
+    def run_pair_learned(self, net: PredictorNet, max_reject_frac=0.05, max_rms_px=0.5) -> dict:
+        """One pair by the learned form, judged; falls back to the plain pair on failure."""
+        fb, rej, rms = C.c_int(), C.c_float(), C.c_float()
+        self._ck(lib().piv_run_pair_learned(self.h, net.h, max_reject_frac, max_rms_px, C.byref(fb), C.byref(rej),
+                                            C.byref(rms)))
+        return {"fell_back": bool(fb.value), "reject_frac": rej.value, "rms_px": rms.value}
 
     def stream(self) -> int:
         s = C.c_void_p()

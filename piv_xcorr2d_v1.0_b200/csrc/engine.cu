@@ -21,6 +21,7 @@
 #include <string>
 #include <vector>
 
+#include "learned.cuh"
 #include "piv_common.cuh"
 
 namespace piv {
@@ -169,6 +170,12 @@ struct piv_engine {
     };
     ResultSlot results[2];
     int result_seq = 0;
+    // learned form (piv_run_pair_learned): its captured graph, keyed by input frames and
+    // net; the upsampled prediction kept for the judge; the judge's two numbers
+    cudaGraphExec_t learned_exec = nullptr;
+    const uint8_t *learned_in1 = nullptr, *learned_in2 = nullptr;
+    const piv_net *learned_net = nullptr;
+    float *d_pred2 = nullptr, *d_judge = nullptr, *h_judge = nullptr;
     std::string err;
     bool timing = false;
     cudaEvent_t ev[6] = {};
@@ -219,6 +226,11 @@ void free_all(piv_engine *e)
 {
     for (int i = 0; i < e->n_graphs; ++i) cudaGraphExecDestroy(e->graphs[i].exec);
     e->n_graphs = 0;
+    if (e->learned_exec) cudaGraphExecDestroy(e->learned_exec);
+    e->learned_exec = nullptr;
+    cudaFree(e->d_pred2);
+    cudaFree(e->d_judge);
+    cudaFreeHost(e->h_judge);
     for (int q = 0; q < 2; ++q) {
         cudaFree(e->d_slot[q][0]);
         cudaFree(e->d_slot[q][1]);
@@ -483,6 +495,49 @@ int do_pair(piv_engine *e, bool with_events)
         }
     }
     mark(3);
+    return PIV_OK;
+}
+
+// Features of the prepared frames at grid 1 into `out` (the predictor input).
+int do_features(piv_engine *e, piv_net *n, float *out)
+{
+    learned::FeatArgs f;
+    f.f1 = e->d_f1 + (size_t)e->my * e->pitch + e->mx;
+    f.f2 = e->d_f2 + (size_t)e->my * e->pitch + e->mx;
+    f.pitch = e->pitch;
+    f.Nx = e->p.Nx;
+    f.Ny = e->p.Ny;
+    f.g = e->grid[0].gg;
+    f.down = learned::net_feature_down(n);
+    f.sums = learned::net_feature_sums(n);
+    f.out = out;
+    CK(learned::launch_features(f, e->stream));
+    return PIV_OK;
+}
+
+// The learned form of a pair up to the judge (captured as one graph): prep, features,
+// network, grid-1 field, upsampling, the grid-2 passes, judge.
+int do_learned(piv_engine *e, piv_net *n)
+{
+    const piv_params &p = e->p;
+    int rc;
+    if ((rc = do_prep(e))) return rc;
+    GridState &g1 = e->grid[0], &g2 = e->grid[1];
+    const int H = g1.gg.Ny_vec, W = g1.gg.Nx_vec;
+    if ((rc = do_features(e, n, learned::net_input(n)))) return rc;
+    CK(learned::net_forward(n, learned::net_input(n), 1, H, W, nullptr, e->stream));
+    CK(learned::launch_field_from_net(learned::net_output(n), g1.gg.Nt_vec, g1.fx, g1.fy, g1.fv, e->stream));
+    if ((rc = do_upsample(e))) return rc;
+    const size_t nt2 = (size_t)g2.gg.Nt_vec;
+    CK(cudaMemcpyAsync(e->d_pred2, g2.fx, nt2 * sizeof(float), cudaMemcpyDeviceToDevice, e->stream));
+    CK(cudaMemcpyAsync(e->d_pred2 + nt2, g2.fy, nt2 * sizeof(float), cudaMemcpyDeviceToDevice, e->stream));
+    for (int j = 0; j < p.Npass2; ++j) {
+        if ((rc = do_pass(e, 1, j))) return rc;
+        if ((rc = do_validate(e, 1, p.Npass2_median, p.minNneigh_p2, p.insert_threshold_p2, p.Npass2_smooth, 1)))
+            return rc;
+    }
+    CK(learned::launch_judge(e->d_pred2, e->d_pred2 + nt2, g2.fx, g2.fy, g2.gg.Nt_vec, e->d_list_n, e->d_judge,
+                             e->stream));
     return PIV_OK;
 }
 
@@ -957,6 +1012,76 @@ int piv_run_pair(piv_engine *e)
     e->grid[0].last_deformed = e->p.Npass1 > 1;
     e->grid[1].has_pass = e->p.Npass2 > 0;
     e->grid[1].last_deformed = true;
+    return PIV_OK;
+}
+
+int piv_net_features(piv_engine *e, piv_net *n, float *d_out)
+{
+    int rc = check_ready(e, true);
+    if (rc) return rc;
+    if (!n || !d_out) return set_err(e, PIV_ERR_ARG, "null net or output");
+    if (e->p.ws_x1 < 8 || e->p.ws_y1 < 8) return set_err(e, PIV_ERR_UNSUPPORTED, "grid-1 windows under 8 px");
+    if ((rc = learned::net_reserve_features(n, e->p.Nx, e->p.Ny))) return set_err(e, rc, "feature scratch");
+    return do_features(e, n, d_out);
+}
+
+int piv_run_pair_learned(piv_engine *e, piv_net *n, float max_reject_frac, float max_rms_px, int *fell_back,
+                         float *reject_frac, float *rms_px)
+{
+    int rc = check_ready(e, false);
+    if (rc) return rc;
+    if (!n) return set_err(e, PIV_ERR_ARG, "null net");
+    if (e->p.Npass2 < 1) return set_err(e, PIV_ERR_STATE, "the learned form needs grid-2 passes (Npass2 > 0)");
+    if (e->p.ws_x1 < 8 || e->p.ws_y1 < 8) return set_err(e, PIV_ERR_UNSUPPORTED, "grid-1 windows under 8 px");
+    if (!xcorr_supported(e->p.ws_x2, e->p.ws_y2)) return set_err(e, PIV_ERR_UNSUPPORTED, "grid-2 window shape not built");
+    if (e->pending_slot >= 0) return set_err(e, PIV_ERR_STATE, "a queued pair is pending: use piv_run_pair");
+    GridState &g1 = e->grid[0], &g2 = e->grid[1];
+    if (!g2.def) {
+        const size_t nd = (size_t)g2.def_pitch * g2.gg.Ny_aug;
+        if ((rc = dalloc(e, &g2.def, nd))) return rc;
+    }
+    if (!e->d_pred2) {
+        if ((rc = dalloc(e, &e->d_pred2, 2 * (size_t)g2.gg.Nt_vec))) return rc;
+        if ((rc = dalloc(e, &e->d_judge, 2))) return rc;
+        if (cudaMallocHost(&e->h_judge, 2 * sizeof(float)) != cudaSuccess)
+            return set_err(e, PIV_ERR_ALLOC, "pinned judge buffer");
+    }
+    if ((rc = learned::net_reserve(n, 1, g1.gg.Ny_vec, g1.gg.Nx_vec))) return set_err(e, rc, "network buffers");
+    if ((rc = learned::net_reserve_features(n, e->p.Nx, e->p.Ny))) return set_err(e, rc, "feature scratch");
+    if (!e->learned_exec || e->learned_in1 != e->d_in1 || e->learned_in2 != e->d_in2 || e->learned_net != n) {
+        if (e->learned_exec) cudaGraphExecDestroy(e->learned_exec);
+        e->learned_exec = nullptr;
+        cudaGraph_t g = nullptr;
+        CK(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
+        rc = do_learned(e, n);
+        cudaError_t ce = cudaStreamEndCapture(e->stream, &g);
+        if (rc) {
+            if (g) cudaGraphDestroy(g);
+            return rc;
+        }
+        if (ce != cudaSuccess) return set_err(e, PIV_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(ce));
+        cudaError_t ie = cudaGraphInstantiate(&e->learned_exec, g, 0);
+        cudaGraphDestroy(g);
+        if (ie != cudaSuccess) return set_err(e, PIV_ERR_CUDA, "graph instantiation failed: %s", cudaGetErrorString(ie));
+        e->learned_in1 = e->d_in1;
+        e->learned_in2 = e->d_in2;
+        e->learned_net = n;
+    }
+    CK(cudaGraphLaunch(e->learned_exec, e->stream));
+    CK(cudaMemcpyAsync(e->h_judge, e->d_judge, 2 * sizeof(float), cudaMemcpyDeviceToHost, e->stream));
+    CK(cudaStreamSynchronize(e->stream));
+    const float rej = e->h_judge[1] / (float)g2.gg.Nt_vec;
+    const float rms = std::sqrt(e->h_judge[0] / (float)g2.gg.Nt_vec);
+    if (reject_frac) *reject_frac = rej;
+    if (rms_px) *rms_px = rms;
+    e->prepared = true;
+    g1.has_pass = true;
+    g1.last_deformed = false;
+    g2.has_pass = true;
+    g2.last_deformed = true;
+    const bool fail = !(rej <= max_reject_frac) || !(rms <= max_rms_px);
+    if (fell_back) *fell_back = fail ? 1 : 0;
+    if (fail) return piv_run_pair(e);
     return PIV_OK;
 }
 

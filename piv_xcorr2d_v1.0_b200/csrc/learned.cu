@@ -1,0 +1,1011 @@
+// learned.cu -- the learned grid-1 predictor: features (cost volume), U-Net forward and
+// backward, loss and Adam, all as hand-written kernels; the net object and its C-ABI.
+// No counterpart in the reference: the plain method's grid-1 passes
+// (X/xcorr2d_multi_grid.cu:1287-1447 driven by X/main.cpp:290-300) are what it replaces.
+//
+// Tensors are [N][C][H][W] FP32.  Weights live as FP32 master copies (Adam state beside
+// them) and as the BF16 copies every convolution reads; biases are FP32.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "learned.cuh"
+#include "piv_b200.h"
+#include "synth_model.h"
+
+namespace piv {
+namespace learned {
+
+constexpr float kSlope = 0.1f;  // LeakyReLU negative slope
+constexpr int kLayers = 13;
+constexpr int kTensors = kLayers + 1;
+
+// Layer i reads tensor `a` (optionally nearest-upsampled x2) concatenated with tensor
+// `b` and writes tensor i + 1.  Tensor 0 is the cost volume.
+struct LayerSpec {
+    int a, ca, b, cb, up, cout, stride, act;
+};
+constexpr LayerSpec kSpec[kLayers] = {
+    {0, 81, -1, 0, 0, 32, 1, 1},    // t1  level 0
+    {1, 32, -1, 0, 0, 32, 1, 1},    // t2  level 0 (skip)
+    {2, 32, -1, 0, 0, 64, 2, 1},    // t3  level 1
+    {3, 64, -1, 0, 0, 64, 1, 1},    // t4  level 1 (skip)
+    {4, 64, -1, 0, 0, 96, 2, 1},    // t5  level 2
+    {5, 96, -1, 0, 0, 96, 1, 1},    // t6  level 2 (skip)
+    {6, 96, -1, 0, 0, 128, 2, 1},   // t7  level 3
+    {7, 128, -1, 0, 0, 128, 1, 1},  // t8  level 3
+    {8, 128, 6, 96, 1, 96, 1, 1},   // t9  level 2: up(t8) ++ t6
+    {9, 96, -1, 0, 0, 96, 1, 1},    // t10 level 2
+    {10, 96, 4, 64, 1, 64, 1, 1},   // t11 level 1: up(t10) ++ t4
+    {11, 64, 2, 32, 1, 32, 1, 1},   // t12 level 0: up(t11) ++ t2
+    {12, 32, -1, 0, 0, 2, 1, 0},    // t13 level 0: head (downsampled px)
+};
+constexpr int kLevel[kTensors] = {0, 0, 0, 1, 1, 2, 2, 3, 3, 2, 2, 1, 0, 0};
+constexpr int kChan[kTensors] = {81, 32, 32, 64, 64, 96, 96, 128, 128, 96, 96, 64, 32, 2};
+
+// ------------------------------------------------------------------------------
+// Features: 4x4 box average and the normalised cost volume.
+// ------------------------------------------------------------------------------
+
+__device__ __forceinline__ float block_sum128(float v, float *red)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    float s = 0.f;
+    if (threadIdx.x == 0)
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[w];
+    return s;
+}
+
+// down[f][y][x] = mean of the 4x4 image block / 255; sums[f] += its total
+__global__ void __launch_bounds__(128) down4_kernel(const uint8_t *f1, const uint8_t *f2, int pitch, int W4, int H4,
+                                                    float *down, double *sums)
+{
+    __shared__ float red[4];
+    const int f = blockIdx.y;
+    const uint8_t *src = f ? f2 : f1;
+    const int q = blockIdx.x * 128 + threadIdx.x;
+    float v = 0.f;
+    if (q < W4 * H4) {
+        const int y = q / W4, x = q - y * W4;
+        const uint8_t *p = src + (size_t)(4 * y) * pitch + 4 * x;
+        int s = 0;
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+#pragma unroll
+            for (int c = 0; c < 4; ++c) s += p[(size_t)r * pitch + c];
+        v = (float)s * (1.0f / (16.0f * 255.0f));
+        down[(size_t)f * W4 * H4 + q] = v;
+    }
+    const float t = block_sum128(v, red);
+    if (threadIdx.x == 0) atomicAdd(sums + f, (double)t);
+}
+
+// One CTA per grid-1 vector.  Window of frame 1: WdxHd downsampled px around the window
+// centre; frame 2 region: the window grown by R on every side.  Outside the image the
+// mean-free frames are 0.
+__global__ void __launch_bounds__(128) cv_kernel(const float *down, const double *sums, int W4, int H4, GridGeom g,
+                                                 float *out)
+{
+    extern __shared__ float sh[];
+    const int ix = blockIdx.x, iy = blockIdx.y;
+    const int Wd = g.ws_x / kDown, Hd = g.ws_y / kDown;
+    const int LW = Wd + 2 * kRadius, LH = Hd + 2 * kRadius;
+    float *s1 = sh, *s2 = sh + Wd * Hd;
+    __shared__ float red[4];
+    __shared__ float energy[2];
+    const float m1 = (float)(sums[0] / ((double)W4 * H4)), m2 = (float)(sums[1] / ((double)W4 * H4));
+    const int cx = ix * g.sp_x - g.Nx_left + g.ws_x / 2, cy = iy * g.sp_y - g.Ny_left + g.ws_y / 2;
+    // nearest block boundary to the centre, in downsampled px
+    const int dcx = (cx + kDown / 2) >> 2, dcy = (cy + kDown / 2) >> 2;
+    const int x0 = dcx - Wd / 2, y0 = dcy - Hd / 2;
+    const float *d1 = down, *d2 = down + (size_t)W4 * H4;
+    for (int e = threadIdx.x; e < Wd * Hd; e += 128) {
+        const int r = e / Wd, c = e - r * Wd;
+        const int y = y0 + r, x = x0 + c;
+        s1[e] = (x >= 0 && x < W4 && y >= 0 && y < H4) ? d1[(size_t)y * W4 + x] - m1 : 0.f;
+    }
+    for (int e = threadIdx.x; e < LW * LH; e += 128) {
+        const int r = e / LW, c = e - r * LW;
+        const int y = y0 - kRadius + r, x = x0 - kRadius + c;
+        s2[e] = (x >= 0 && x < W4 && y >= 0 && y < H4) ? d2[(size_t)y * W4 + x] - m2 : 0.f;
+    }
+    __syncthreads();
+    // window energies (frame 2 at zero shift)
+    float e1 = 0.f, e2 = 0.f;
+    for (int e = threadIdx.x; e < Wd * Hd; e += 128) {
+        const int r = e / Wd, c = e - r * Wd;
+        const float a = s1[e], b = s2[(r + kRadius) * LW + c + kRadius];
+        e1 += a * a;
+        e2 += b * b;
+    }
+    const float t1 = block_sum128(e1, red);
+    __syncthreads();
+    const float t2 = block_sum128(e2, red);
+    if (threadIdx.x == 0) {
+        energy[0] = t1;
+        energy[1] = t2;
+    }
+    __syncthreads();
+    const int t = threadIdx.x;
+    if (t < kInChannels) {
+        const int dy = t / kShifts, dx = t - dy * kShifts;  // shift + R
+        float acc = 0.f;
+        for (int r = 0; r < Hd; ++r) {
+            const float *a = s1 + r * Wd, *b = s2 + (r + dy) * LW + dx;
+            for (int c = 0; c < Wd; ++c) acc = fmaf(a[c], b[c], acc);
+        }
+        const float den = energy[0] * energy[1];
+        const float v = den > 0.f ? acc * rsqrtf(den) : 0.f;
+        out[((size_t)t * g.Ny_vec + iy) * g.Nx_vec + ix] = v;
+    }
+}
+
+size_t feature_scratch_floats(int Nx, int Ny) { return (size_t)2 * (Nx / kDown) * (Ny / kDown); }
+
+cudaError_t launch_features(const FeatArgs &a, cudaStream_t s)
+{
+    const int W4 = a.Nx / kDown, H4 = a.Ny / kDown;
+    if (W4 < 1 || H4 < 1 || a.g.ws_x < 2 * kDown || a.g.ws_y < 2 * kDown) return cudaErrorInvalidValue;
+    cudaError_t e = cudaMemsetAsync(a.sums, 0, 2 * sizeof(double), s);
+    if (e != cudaSuccess) return e;
+    down4_kernel<<<dim3((W4 * H4 + 127) / 128, 2), 128, 0, s>>>(a.f1, a.f2, a.pitch, W4, H4, a.down, a.sums);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    const int Wd = a.g.ws_x / kDown, Hd = a.g.ws_y / kDown;
+    const size_t smem = sizeof(float) * ((size_t)Wd * Hd + (size_t)(Wd + 2 * kRadius) * (Hd + 2 * kRadius));
+    if (smem > 48 * 1024) return cudaErrorInvalidValue;
+    cv_kernel<<<dim3(a.g.Nx_vec, a.g.Ny_vec), 128, smem, s>>>(a.down, a.sums, W4, H4, a.g, a.out);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------------------
+// Convolutions (3x3, padding 1, stride 1 or 2).  The input is tensor a (optionally read
+// through a nearest x2 upsampling) concatenated with tensor b along channels.
+// ------------------------------------------------------------------------------
+
+struct ConvIn {
+    const float *a, *b;
+    int ca, cb, up;
+    int Hin, Win;  // resolution of the (upsampled) input
+    int Ha, Wa;    // resolution of a as stored
+};
+
+struct ConvFwd {
+    ConvIn in;
+    int N, Ho, Wo, stride;
+    const __nv_bfloat16 *w;
+    const float *bias;
+    int cout;
+    float *out;
+    int act;
+};
+
+// tap offsets of output pixel (oy, ox): into a (upsampled or not) and into b
+__device__ __forceinline__ void conv_taps(const ConvIn &c, int oy, int ox, int stride, bool live, int (&oa)[9],
+                                          int (&ob)[9])
+{
+#pragma unroll
+    for (int ky = 0; ky < 3; ++ky)
+#pragma unroll
+        for (int kx = 0; kx < 3; ++kx) {
+            const int y = oy * stride + ky - 1, x = ox * stride + kx - 1;
+            const bool ok = live && y >= 0 && y < c.Hin && x >= 0 && x < c.Win;
+            ob[ky * 3 + kx] = ok ? y * c.Win + x : -1;
+            oa[ky * 3 + kx] = ok ? (c.up ? (y >> 1) * c.Wa + (x >> 1) : y * c.Win + x) : -1;
+        }
+}
+
+__device__ __forceinline__ void conv_gather(const ConvIn &c, int n, int ci, const int (&oa)[9], const int (&ob)[9],
+                                            float (&x)[9])
+{
+    if (ci < c.ca) {
+        const float *src = c.a + ((size_t)n * c.ca + ci) * c.Ha * c.Wa;
+#pragma unroll
+        for (int t = 0; t < 9; ++t) x[t] = oa[t] >= 0 ? __ldg(src + oa[t]) : 0.f;
+    } else {
+        const float *src = c.b + ((size_t)n * c.cb + (ci - c.ca)) * c.Hin * c.Win;
+#pragma unroll
+        for (int t = 0; t < 9; ++t) x[t] = ob[t] >= 0 ? __ldg(src + ob[t]) : 0.f;
+    }
+}
+
+// Thread per output pixel, COB output channels per CTA; weights staged through shared
+// memory CIC input channels at a time, laid [ci][tap][co] so every FMA reads a broadcast.
+template <int COB>
+__global__ void __launch_bounds__(128) conv_fwd_kernel(const ConvFwd c)
+{
+    constexpr int CIC = 8;
+    __shared__ __align__(16) float ws[CIC][9][COB];
+    const int n = blockIdx.z, co0 = blockIdx.y * COB;
+    const int p = blockIdx.x * 128 + threadIdx.x;
+    const bool live = p < c.Ho * c.Wo;
+    const int oy = live ? p / c.Wo : 0, ox = live ? p - oy * c.Wo : 0;
+    const int cin = c.in.ca + c.in.cb;
+    int oa[9], ob[9];
+    conv_taps(c.in, oy, ox, c.stride, live, oa, ob);
+    float acc[COB];
+#pragma unroll
+    for (int k = 0; k < COB; ++k) acc[k] = 0.f;
+    for (int ci0 = 0; ci0 < cin; ci0 += CIC) {
+        __syncthreads();
+        for (int e = threadIdx.x; e < CIC * 9 * COB; e += 128) {
+            const int co = e % COB, r = e / COB, tap = r % 9, ci = r / 9;
+            float wv = 0.f;
+            if (ci0 + ci < cin && co0 + co < c.cout)
+                wv = __bfloat162float(c.w[((size_t)(co0 + co) * cin + ci0 + ci) * 9 + tap]);
+            ws[ci][tap][co] = wv;
+        }
+        __syncthreads();
+        const int nci = min(CIC, cin - ci0);
+#pragma unroll 1
+        for (int ci = 0; ci < nci; ++ci) {
+            float x[9];
+            conv_gather(c.in, n, ci0 + ci, oa, ob, x);
+#pragma unroll
+            for (int t = 0; t < 9; ++t)
+#pragma unroll
+                for (int k = 0; k < COB; ++k) acc[k] = fmaf(ws[ci][t][k], x[t], acc[k]);
+        }
+    }
+    if (!live) return;
+#pragma unroll
+    for (int k = 0; k < COB; ++k) {
+        const int co = co0 + k;
+        if (co >= c.cout) break;
+        float v = acc[k] + c.bias[co];
+        if (c.act) v = v > 0.f ? v : kSlope * v;
+        c.out[((size_t)n * c.cout + co) * c.Ho * c.Wo + p] = v;
+    }
+}
+
+// dIn of the concatenated (upsampled) input, [N][ca+cb][Hin][Win], overwritten.
+struct ConvBwdData {
+    int N, cin, Hin, Win, Ho, Wo, stride, cout;
+    const __nv_bfloat16 *w;
+    const float *g;  // [N][cout][Ho][Wo], activation gradient already applied
+    float *din;
+};
+
+template <int CIB>
+__global__ void __launch_bounds__(128) conv_bwd_data_kernel(const ConvBwdData c)
+{
+    constexpr int COC = 8;
+    __shared__ __align__(16) float ws[COC][9][CIB];
+    const int n = blockIdx.z, ci0 = blockIdx.y * CIB;
+    const int p = blockIdx.x * 128 + threadIdx.x;
+    const bool live = p < c.Hin * c.Win;
+    const int y = live ? p / c.Win : 0, x = live ? p - y * c.Win : 0;
+    // output pixel fed by each tap: y = oy*s + ky - 1  =>  oy = (y + 1 - ky) / s
+    int og[9];
+#pragma unroll
+    for (int ky = 0; ky < 3; ++ky)
+#pragma unroll
+        for (int kx = 0; kx < 3; ++kx) {
+            const int ny = y + 1 - ky, nx = x + 1 - kx;
+            int oy = -1, ox = -1;
+            if (c.stride == 1) {
+                oy = ny;
+                ox = nx;
+            } else if (ny >= 0 && nx >= 0 && !(ny & 1) && !(nx & 1)) {
+                oy = ny >> 1;
+                ox = nx >> 1;
+            }
+            const bool ok = live && oy >= 0 && oy < c.Ho && ox >= 0 && ox < c.Wo;
+            og[ky * 3 + kx] = ok ? oy * c.Wo + ox : -1;
+        }
+    float acc[CIB];
+#pragma unroll
+    for (int k = 0; k < CIB; ++k) acc[k] = 0.f;
+    for (int co0 = 0; co0 < c.cout; co0 += COC) {
+        __syncthreads();
+        for (int e = threadIdx.x; e < COC * 9 * CIB; e += 128) {
+            const int ci = e % CIB, r = e / CIB, tap = r % 9, co = r / 9;
+            float wv = 0.f;
+            if (co0 + co < c.cout && ci0 + ci < c.cin)
+                wv = __bfloat162float(c.w[((size_t)(co0 + co) * c.cin + ci0 + ci) * 9 + tap]);
+            ws[co][tap][ci] = wv;
+        }
+        __syncthreads();
+        const int nco = min(COC, c.cout - co0);
+#pragma unroll 1
+        for (int co = 0; co < nco; ++co) {
+            const float *src = c.g + ((size_t)n * c.cout + co0 + co) * c.Ho * c.Wo;
+            float gv[9];
+#pragma unroll
+            for (int t = 0; t < 9; ++t) gv[t] = og[t] >= 0 ? __ldg(src + og[t]) : 0.f;
+#pragma unroll
+            for (int t = 0; t < 9; ++t)
+#pragma unroll
+                for (int k = 0; k < CIB; ++k) acc[k] = fmaf(ws[co][t][k], gv[t], acc[k]);
+        }
+    }
+    if (!live) return;
+#pragma unroll
+    for (int k = 0; k < CIB; ++k) {
+        const int ci = ci0 + k;
+        if (ci >= c.cin) break;
+        c.din[((size_t)n * c.cin + ci) * c.Hin * c.Win + p] = acc[k];
+    }
+}
+
+// dW[co][ci][tap] and db[co]: one CTA per (input channel, COC output channels), threads
+// over the N*Ho*Wo output pixels, then a block reduction.  Overwrites its outputs.
+struct ConvBwdW {
+    ConvIn in;
+    int N, Ho, Wo, stride, cout;
+    const float *g;
+    float *dw, *db;
+};
+
+template <int COC>
+__global__ void __launch_bounds__(256) conv_bwd_w_kernel(const ConvBwdW c)
+{
+    constexpr int NV = COC * 10;  // 9 taps + bias per output channel
+    __shared__ float red[8][NV];
+    const int ci = blockIdx.x, co0 = blockIdx.y * COC;
+    const int cin = c.in.ca + c.in.cb;
+    const int HW = c.Ho * c.Wo, npix = c.N * HW;
+    float acc[COC][10];
+#pragma unroll
+    for (int k = 0; k < COC; ++k)
+#pragma unroll
+        for (int t = 0; t < 10; ++t) acc[k][t] = 0.f;
+    for (int q = threadIdx.x; q < npix; q += 256) {
+        const int n = q / HW, p = q - n * HW;
+        const int oy = p / c.Wo, ox = p - oy * c.Wo;
+        int oa[9], ob[9];
+        conv_taps(c.in, oy, ox, c.stride, true, oa, ob);
+        float x[9];
+        conv_gather(c.in, n, ci, oa, ob, x);
+#pragma unroll
+        for (int k = 0; k < COC; ++k) {
+            const int co = co0 + k;
+            const float gv = co < c.cout ? __ldg(c.g + ((size_t)n * c.cout + co) * HW + p) : 0.f;
+#pragma unroll
+            for (int t = 0; t < 9; ++t) acc[k][t] = fmaf(gv, x[t], acc[k][t]);
+            acc[k][9] += gv;
+        }
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < COC; ++k)
+#pragma unroll
+        for (int t = 0; t < 10; ++t) {
+            float v = acc[k][t];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            if (lane == 0) red[warp][k * 10 + t] = v;
+        }
+    __syncthreads();
+    for (int e = threadIdx.x; e < NV; e += 256) {
+        float s = 0.f;
+#pragma unroll
+        for (int w = 0; w < 8; ++w) s += red[w][e];
+        const int k = e / 10, t = e - k * 10, co = co0 + k;
+        if (co >= c.cout) continue;
+        if (t < 9) c.dw[((size_t)co * cin + ci) * 9 + t] = s;
+        else if (ci == 0) c.db[co] = s;
+    }
+}
+
+// g *= LeakyReLU'(pre-activation), read from the layer output's sign
+__global__ void act_bwd_kernel(float *g, const float *out, size_t n)
+{
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n && !(out[i] > 0.f)) g[i] *= kSlope;
+}
+
+// Route dIn of a concatenated input back: ga (+=, summing the 2x2 fine pixels of each
+// coarse pixel when a was upsampled) and gb (+=).
+__global__ void split_grad_kernel(const float *din, int N, int ca, int cb, int up, int Hin, int Win, int Ha, int Wa,
+                                  float *ga, float *gb)
+{
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const size_t na = ga ? (size_t)N * ca * Ha * Wa : 0, nb = gb ? (size_t)N * cb * Hin * Win : 0;
+    const int cin = ca + cb;
+    if (i < na) {
+        const int X = (int)(i % Wa);
+        size_t r = i / Wa;
+        const int Y = (int)(r % Ha);
+        r /= Ha;
+        const int ch = (int)(r % ca), n = (int)(r / ca);
+        const float *src = din + ((size_t)n * cin + ch) * Hin * Win;
+        float s;
+        if (up) {
+            s = 0.f;
+            for (int dy = 0; dy < 2; ++dy)
+                for (int dx = 0; dx < 2; ++dx) {
+                    const int y = 2 * Y + dy, x = 2 * X + dx;
+                    if (y < Hin && x < Win) s += src[y * Win + x];
+                }
+        } else {
+            s = src[Y * Win + X];
+        }
+        ga[i] += s;
+    } else if (i < na + nb) {
+        const size_t j = i - na;
+        const int x = (int)(j % Win);
+        size_t r = j / Win;
+        const int y = (int)(r % Hin);
+        r /= Hin;
+        const int ch = (int)(r % cb), n = (int)(r / cb);
+        gb[j] += din[((size_t)n * cin + ca + ch) * Hin * Win + y * Win + x];
+    }
+}
+
+// Charbonnier loss on the head (downsampled px): sum over masked vectors of
+// sqrt(e^2 + eps^2) - eps per component, times inv_count; its gradient into gpred.
+__global__ void loss_kernel(const float *pred, const float *label, const float *mask, int N, int HW, float inv_count,
+                            float *gpred, float *loss)
+{
+    constexpr float eps = 0.01f;
+    __shared__ float red[8];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    float l = 0.f;
+    if (i < N * HW) {
+        const int n = i / HW, p = i - n * HW;
+        const float m = mask[i] * inv_count;
+#pragma unroll
+        for (int ch = 0; ch < 2; ++ch) {
+            const size_t o = ((size_t)n * 2 + ch) * HW + p;
+            const float e = pred[o] - label[o];
+            const float r = sqrtf(e * e + eps * eps);
+            l += m * (r - eps);
+            gpred[o] = m * e / r;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) l += __shfl_xor_sync(0xffffffffu, l, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = l;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float s = 0.f;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[w];
+        atomicAdd(loss, s);
+    }
+}
+
+// Adam (Kingma & Ba, 2015) with bias correction; refreshes the BF16 copies.
+__global__ void adam_kernel(float *p, const float *g, float *m, float *v, __nv_bfloat16 *pb, size_t n, float lr,
+                            float b1, float b2, float eps, float c1, float c2)
+{
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float gi = g[i];
+    const float mi = b1 * m[i] + (1.f - b1) * gi, vi = b2 * v[i] + (1.f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    const float pi = p[i] - lr * (mi * c1) / (sqrtf(vi * c2) + eps);
+    p[i] = pi;
+    pb[i] = __float2bfloat16_rn(pi);
+}
+
+__global__ void to_bf16_kernel(const float *p, __nv_bfloat16 *pb, size_t n)
+{
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) pb[i] = __float2bfloat16_rn(p[i]);
+}
+
+__global__ void field_from_net_kernel(const float *out, int Nt, float *fx, float *fy, uint8_t *fv)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= Nt) return;
+    fx[i] = kOutScale * out[i];
+    fy[i] = kOutScale * out[Nt + i];
+    fv[i] = 1;
+}
+
+cudaError_t launch_field_from_net(const float *out, int Nt, float *fx, float *fy, uint8_t *fv, cudaStream_t s)
+{
+    field_from_net_kernel<<<(Nt + 255) / 256, 256, 0, s>>>(out, Nt, fx, fy, fv);
+    return cudaGetLastError();
+}
+
+__global__ void __launch_bounds__(1024) judge_kernel(const float *px, const float *py, const float *fx,
+                                                     const float *fy, int Nt, const int *list_n, float *judge)
+{
+    __shared__ float red[32];
+    float s = 0.f;
+    for (int i = threadIdx.x; i < Nt; i += 1024) {
+        const float dx = px[i] - fx[i], dy = py[i] - fy[i];
+        s += dx * dx + dy * dy;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        float v = red[threadIdx.x];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (threadIdx.x == 0) {
+            judge[0] = v;
+            judge[1] = (float)*list_n;
+        }
+    }
+}
+
+cudaError_t launch_judge(const float *px, const float *py, const float *fx, const float *fy, int Nt,
+                         const int *list_n, float *judge, cudaStream_t s)
+{
+    judge_kernel<<<1, 1024, 0, s>>>(px, py, fx, fy, Nt, list_n, judge);
+    return cudaGetLastError();
+}
+
+}  // namespace learned
+}  // namespace piv
+
+using namespace piv;
+using namespace piv::learned;
+
+struct piv_net {
+    int device = 0;
+    size_t n_params = 0;
+    size_t w_off[kLayers] = {}, b_off[kLayers] = {};
+    float *params = nullptr, *grads = nullptr, *adam_m = nullptr, *adam_v = nullptr;
+    __nv_bfloat16 *wbf = nullptr;
+    int step = 0;
+    // activations for (aN, aH, aW)
+    int aN = 0, aH = 0, aW = 0;
+    int lh[4] = {}, lw[4] = {};
+    size_t t_off[kTensors] = {};
+    size_t act_floats = 0, din_floats = 0;
+    float *act = nullptr, *gact = nullptr, *din = nullptr;
+    float *d_loss = nullptr, *h_loss = nullptr;
+    // features scratch
+    float *fdown = nullptr;
+    double *fsums = nullptr;
+    size_t fcap = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+};
+
+namespace {
+
+int net_err(piv_net *n, int code, const char *msg)
+{
+    if (n) n->err = msg;
+    return code;
+}
+
+#define NCK(call)                                                                   \
+    do {                                                                            \
+        cudaError_t _e = (call);                                                    \
+        if (_e != cudaSuccess) return net_err(n, PIV_ERR_CUDA, cudaGetErrorString(_e)); \
+    } while (0)
+
+void layout(piv_net *n, int N, int H, int W)
+{
+    n->lh[0] = H;
+    n->lw[0] = W;
+    for (int l = 1; l < 4; ++l) {
+        n->lh[l] = (n->lh[l - 1] + 1) / 2;
+        n->lw[l] = (n->lw[l - 1] + 1) / 2;
+    }
+    size_t off = 0;
+    for (int t = 0; t < kTensors; ++t) {
+        n->t_off[t] = off;
+        const size_t sz = (size_t)N * kChan[t] * n->lh[kLevel[t]] * n->lw[kLevel[t]];
+        off += (sz + 31) & ~(size_t)31;
+    }
+    n->act_floats = off;
+    size_t dmax = 0;
+    for (int i = 0; i < kLayers; ++i) {
+        const LayerSpec &s = kSpec[i];
+        const int lin = s.up ? kLevel[s.b] : kLevel[s.a];
+        dmax = std::max(dmax, (size_t)N * (s.ca + s.cb) * n->lh[lin] * n->lw[lin]);
+    }
+    n->din_floats = dmax;
+}
+
+ConvIn conv_in(piv_net *n, const float *base, int i, int N)
+{
+    (void)N;
+    const LayerSpec &s = kSpec[i];
+    ConvIn c;
+    c.a = base + n->t_off[s.a];
+    c.b = s.b >= 0 ? base + n->t_off[s.b] : nullptr;
+    c.ca = s.ca;
+    c.cb = s.cb;
+    c.up = s.up;
+    const int la = kLevel[s.a];
+    const int lin = s.up ? kLevel[s.b] : la;
+    c.Hin = n->lh[lin];
+    c.Win = n->lw[lin];
+    c.Ha = n->lh[la];
+    c.Wa = n->lw[la];
+    return c;
+}
+
+cudaError_t forward_layers(piv_net *n, float *act, int N, cudaStream_t s)
+{
+    for (int i = 0; i < kLayers; ++i) {
+        const LayerSpec &sp = kSpec[i];
+        ConvFwd c;
+        c.in = conv_in(n, act, i, N);
+        const int lo = kLevel[i + 1];
+        c.N = N;
+        c.Ho = n->lh[lo];
+        c.Wo = n->lw[lo];
+        c.stride = sp.stride;
+        c.w = n->wbf + n->w_off[i];
+        c.bias = n->params + n->b_off[i];
+        c.cout = sp.cout;
+        c.out = act + n->t_off[i + 1];
+        c.act = sp.act;
+        const int px = c.Ho * c.Wo;
+        if (sp.cout % 32 == 0) {
+            conv_fwd_kernel<32><<<dim3((px + 127) / 128, sp.cout / 32, N), 128, 0, s>>>(c);
+        } else {
+            conv_fwd_kernel<2><<<dim3((px + 127) / 128, (sp.cout + 1) / 2, N), 128, 0, s>>>(c);
+        }
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+}  // namespace
+
+namespace piv {
+namespace learned {
+
+int net_reserve(piv_net *n, int N, int H, int W)
+{
+    if (!n || N < 1 || H < 1 || W < 1) return PIV_ERR_ARG;
+    if (n->act && n->aN == N && n->aH == H && n->aW == W) return PIV_OK;
+    cudaSetDevice(n->device);
+    const size_t old_act = n->act ? n->act_floats : 0, old_din = n->act ? n->din_floats : 0;
+    layout(n, N, H, W);
+    if (n->act_floats > old_act || n->din_floats > old_din || !n->act) {
+        cudaFree(n->act);
+        cudaFree(n->gact);
+        cudaFree(n->din);
+        n->act = n->gact = n->din = nullptr;
+        NCK(cudaMalloc(&n->act, n->act_floats * sizeof(float)));
+        NCK(cudaMalloc(&n->gact, n->act_floats * sizeof(float)));
+        NCK(cudaMalloc(&n->din, n->din_floats * sizeof(float)));
+    } else {
+        n->act_floats = std::max(n->act_floats, old_act);
+        n->din_floats = std::max(n->din_floats, old_din);
+    }
+    n->aN = N;
+    n->aH = H;
+    n->aW = W;
+    return PIV_OK;
+}
+
+float *net_input(piv_net *n) { return n->act + n->t_off[0]; }
+const float *net_output(piv_net *n) { return n->act + n->t_off[kTensors - 1]; }
+
+cudaError_t net_forward(piv_net *n, const float *in, int N, int H, int W, float *out, cudaStream_t s)
+{
+    if (!n->act || n->aN != N || n->aH != H || n->aW != W) return cudaErrorInvalidValue;
+    float *t0 = n->act + n->t_off[0];
+    const size_t nin = (size_t)N * kInChannels * H * W;
+    cudaError_t e;
+    if (in != t0 && (e = cudaMemcpyAsync(t0, in, nin * sizeof(float), cudaMemcpyDeviceToDevice, s)) != cudaSuccess)
+        return e;
+    if ((e = forward_layers(n, n->act, N, s)) != cudaSuccess) return e;
+    const float *t13 = n->act + n->t_off[kTensors - 1];
+    if (out && out != t13)
+        return cudaMemcpyAsync(out, t13, (size_t)N * 2 * H * W * sizeof(float), cudaMemcpyDeviceToDevice, s);
+    return cudaSuccess;
+}
+
+int net_reserve_features(piv_net *n, int Nx, int Ny)
+{
+    const size_t need = feature_scratch_floats(Nx, Ny);
+    if (n->fdown && n->fcap >= need) return PIV_OK;
+    cudaSetDevice(n->device);
+    cudaFree(n->fdown);
+    n->fdown = nullptr;
+    NCK(cudaMalloc(&n->fdown, need * sizeof(float)));
+    if (!n->fsums) NCK(cudaMalloc(&n->fsums, 2 * sizeof(double)));
+    n->fcap = need;
+    return PIV_OK;
+}
+
+float *net_feature_down(piv_net *n) { return n->fdown; }
+double *net_feature_sums(piv_net *n) { return n->fsums; }
+
+}  // namespace learned
+}  // namespace piv
+
+// ------------------------------------------------------------------------------
+// C-ABI
+// ------------------------------------------------------------------------------
+extern "C" {
+
+int piv_net_create(uint64_t seed, piv_net **out)
+{
+    if (!out) return PIV_ERR_ARG;
+    *out = nullptr;
+    piv_net *n = new piv_net;
+    cudaGetDevice(&n->device);
+    size_t off = 0;
+    for (int i = 0; i < kLayers; ++i) {
+        n->w_off[i] = off;
+        off += (size_t)kSpec[i].cout * (kSpec[i].ca + kSpec[i].cb) * 9;
+        n->b_off[i] = off;
+        off += kSpec[i].cout;
+    }
+    n->n_params = off;
+    // He-uniform weights for LeakyReLU (bound sqrt(6 / ((1 + slope^2) fan_in))), a head
+    // scaled by 0.1, zero biases; Philox stream 4 of the seed
+    std::vector<float> h(off, 0.f);
+    for (int i = 0; i < kLayers; ++i) {
+        const int fan_in = (kSpec[i].ca + kSpec[i].cb) * 9;
+        double bound = std::sqrt(6.0 / ((1.0 + kSlope * kSlope) * fan_in));
+        if (!kSpec[i].act) bound *= 0.1;
+        const size_t nw = (size_t)kSpec[i].cout * fan_in;
+        for (size_t k = 0; k < nw; ++k) {
+            const U4 r = philox((uint32_t)k, (uint32_t)i, 4, 0, seed);
+            h[n->w_off[i] + k] = (float)((2.0 * u01(r.v[0]) - 1.0) * bound);
+        }
+    }
+    int rc = PIV_OK;
+    auto fail = [&](int code) {
+        rc = code;
+        cudaFree(n->params);
+        cudaFree(n->grads);
+        cudaFree(n->adam_m);
+        cudaFree(n->adam_v);
+        cudaFree(n->wbf);
+        cudaFree(n->d_loss);
+        if (n->h_loss) cudaFreeHost(n->h_loss);
+        if (n->stream) cudaStreamDestroy(n->stream);
+        delete n;
+        return rc;
+    };
+    if (cudaMalloc(&n->params, off * sizeof(float)) != cudaSuccess ||
+        cudaMalloc(&n->grads, off * sizeof(float)) != cudaSuccess ||
+        cudaMalloc(&n->adam_m, off * sizeof(float)) != cudaSuccess ||
+        cudaMalloc(&n->adam_v, off * sizeof(float)) != cudaSuccess ||
+        cudaMalloc(&n->wbf, off * sizeof(__nv_bfloat16)) != cudaSuccess ||
+        cudaMalloc(&n->d_loss, sizeof(float)) != cudaSuccess ||
+        cudaMallocHost(&n->h_loss, sizeof(float)) != cudaSuccess ||
+        cudaStreamCreate(&n->stream) != cudaSuccess)  // blocking: ordered after default-stream work
+        return fail(PIV_ERR_CUDA);
+    if (cudaMemcpy(n->params, h.data(), off * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemset(n->adam_m, 0, off * sizeof(float)) != cudaSuccess ||
+        cudaMemset(n->adam_v, 0, off * sizeof(float)) != cudaSuccess ||
+        cudaMemset(n->grads, 0, off * sizeof(float)) != cudaSuccess)
+        return fail(PIV_ERR_CUDA);
+    to_bf16_kernel<<<(unsigned)((off + 255) / 256), 256, 0, n->stream>>>(n->params, n->wbf, off);
+    if (cudaStreamSynchronize(n->stream) != cudaSuccess) return fail(PIV_ERR_CUDA);
+    *out = n;
+    return PIV_OK;
+}
+
+int piv_net_destroy(piv_net *n)
+{
+    if (!n) return PIV_ERR_ARG;
+    cudaSetDevice(n->device);
+    if (n->stream) cudaStreamSynchronize(n->stream);
+    cudaFree(n->params);
+    cudaFree(n->grads);
+    cudaFree(n->adam_m);
+    cudaFree(n->adam_v);
+    cudaFree(n->wbf);
+    cudaFree(n->act);
+    cudaFree(n->gact);
+    cudaFree(n->din);
+    cudaFree(n->d_loss);
+    cudaFree(n->fdown);
+    cudaFree(n->fsums);
+    if (n->h_loss) cudaFreeHost(n->h_loss);
+    if (n->stream) cudaStreamDestroy(n->stream);
+    delete n;
+    return PIV_OK;
+}
+
+const char *piv_net_last_error(const piv_net *n) { return n ? n->err.c_str() : "null net"; }
+
+int piv_net_num_params(const piv_net *n, int64_t *count)
+{
+    if (!n || !count) return PIV_ERR_ARG;
+    *count = (int64_t)n->n_params;
+    return PIV_OK;
+}
+
+int piv_net_layout(int layer, int *cin, int *cout, int *stride, int *weight_offset, int *bias_offset)
+{
+    if (layer < 0 || layer >= kLayers) return PIV_ERR_ARG;
+    size_t off = 0;
+    for (int i = 0; i < layer; ++i) off += (size_t)kSpec[i].cout * ((kSpec[i].ca + kSpec[i].cb) * 9 + 1);
+    const LayerSpec &s = kSpec[layer];
+    if (cin) *cin = s.ca + s.cb;
+    if (cout) *cout = s.cout;
+    if (stride) *stride = s.stride;
+    if (weight_offset) *weight_offset = (int)off;
+    if (bias_offset) *bias_offset = (int)(off + (size_t)s.cout * (s.ca + s.cb) * 9);
+    return PIV_OK;
+}
+
+int piv_net_get_params(piv_net *n, float *host, int64_t count)
+{
+    if (!n || !host || count != (int64_t)n->n_params) return PIV_ERR_ARG;
+    cudaSetDevice(n->device);
+    NCK(cudaStreamSynchronize(n->stream));
+    NCK(cudaMemcpy(host, n->params, n->n_params * sizeof(float), cudaMemcpyDeviceToHost));
+    return PIV_OK;
+}
+
+int piv_net_set_params(piv_net *n, const float *host, int64_t count)
+{
+    if (!n || !host || count != (int64_t)n->n_params) return PIV_ERR_ARG;
+    cudaSetDevice(n->device);
+    NCK(cudaStreamSynchronize(n->stream));
+    NCK(cudaMemcpy(n->params, host, n->n_params * sizeof(float), cudaMemcpyHostToDevice));
+    NCK(cudaMemset(n->adam_m, 0, n->n_params * sizeof(float)));
+    NCK(cudaMemset(n->adam_v, 0, n->n_params * sizeof(float)));
+    n->step = 0;
+    to_bf16_kernel<<<(unsigned)((n->n_params + 255) / 256), 256, 0, n->stream>>>(n->params, n->wbf, n->n_params);
+    NCK(cudaGetLastError());
+    NCK(cudaStreamSynchronize(n->stream));
+    return PIV_OK;
+}
+
+int piv_net_get_grads(piv_net *n, float *host, int64_t count)
+{
+    if (!n || !host || count != (int64_t)n->n_params) return PIV_ERR_ARG;
+    cudaSetDevice(n->device);
+    NCK(cudaStreamSynchronize(n->stream));
+    NCK(cudaMemcpy(host, n->grads, n->n_params * sizeof(float), cudaMemcpyDeviceToHost));
+    return PIV_OK;
+}
+
+// weights file: "PIVNET01", uint64 count, count float32 (little-endian)
+int piv_net_save(piv_net *n, const char *path)
+{
+    if (!n || !path) return PIV_ERR_ARG;
+    std::vector<float> h(n->n_params);
+    int rc = piv_net_get_params(n, h.data(), (int64_t)h.size());
+    if (rc) return rc;
+    FILE *f = fopen(path, "wb");
+    if (!f) return net_err(n, PIV_ERR_IO, "cannot open the weights file for writing");
+    const uint64_t cnt = h.size();
+    bool ok = fwrite("PIVNET01", 1, 8, f) == 8 && fwrite(&cnt, 8, 1, f) == 1 &&
+              fwrite(h.data(), sizeof(float), h.size(), f) == h.size();
+    ok = (fclose(f) == 0) && ok;
+    return ok ? PIV_OK : net_err(n, PIV_ERR_IO, "short write of the weights file");
+}
+
+int piv_net_load(piv_net *n, const char *path)
+{
+    if (!n || !path) return PIV_ERR_ARG;
+    FILE *f = fopen(path, "rb");
+    if (!f) return net_err(n, PIV_ERR_IO, "cannot open the weights file");
+    char magic[8];
+    uint64_t cnt = 0;
+    std::vector<float> h;
+    bool ok = fread(magic, 1, 8, f) == 8 && memcmp(magic, "PIVNET01", 8) == 0 && fread(&cnt, 8, 1, f) == 1 &&
+              cnt == n->n_params;
+    if (ok) {
+        h.resize(cnt);
+        ok = fread(h.data(), sizeof(float), cnt, f) == cnt;
+    }
+    fclose(f);
+    if (!ok) return net_err(n, PIV_ERR_IO, "not a weights file of this network");
+    return piv_net_set_params(n, h.data(), (int64_t)cnt);
+}
+
+int piv_net_forward(piv_net *n, const float *d_in, int N, int H, int W, float *d_out, void *stream)
+{
+    if (!n || !d_in || !d_out) return PIV_ERR_ARG;
+    cudaSetDevice(n->device);
+    int rc = net_reserve(n, N, H, W);
+    if (rc) return rc;
+    cudaStream_t s = stream ? (cudaStream_t)stream : n->stream;
+    NCK(net_forward(n, d_in, N, H, W, d_out, s));
+    return PIV_OK;
+}
+
+int piv_net_loss_grad(piv_net *n, const float *d_in, const float *d_label, const float *d_mask, int N, int H, int W,
+                      float *loss)
+{
+    if (!n || !d_in || !d_label || !d_mask) return PIV_ERR_ARG;
+    cudaSetDevice(n->device);
+    int rc = net_reserve(n, N, H, W);
+    if (rc) return rc;
+    cudaStream_t s = n->stream;
+    NCK(net_forward(n, d_in, N, H, W, nullptr, s));
+    // mask count on the device would need a reduction first; the host counts instead
+    std::vector<float> hm((size_t)N * H * W);
+    NCK(cudaMemcpyAsync(hm.data(), d_mask, hm.size() * sizeof(float), cudaMemcpyDeviceToHost, s));
+    NCK(cudaStreamSynchronize(s));
+    double cnt = 0;
+    for (float v : hm) cnt += v;
+    const float inv = cnt > 0 ? (float)(1.0 / cnt) : 0.f;
+    NCK(cudaMemsetAsync(n->gact, 0, n->act_floats * sizeof(float), s));
+    NCK(cudaMemsetAsync(n->d_loss, 0, sizeof(float), s));
+    const int HW = H * W;
+    float *pred = n->act + n->t_off[kTensors - 1], *gpred = n->gact + n->t_off[kTensors - 1];
+    loss_kernel<<<(N * HW + 255) / 256, 256, 0, s>>>(pred, d_label, d_mask, N, HW, inv, gpred, n->d_loss);
+    NCK(cudaGetLastError());
+    for (int i = kLayers - 1; i >= 0; --i) {
+        const LayerSpec &sp = kSpec[i];
+        const int lo = kLevel[i + 1];
+        const int Ho = n->lh[lo], Wo = n->lw[lo];
+        float *g = n->gact + n->t_off[i + 1];
+        const float *o = n->act + n->t_off[i + 1];
+        const size_t no = (size_t)N * sp.cout * Ho * Wo;
+        if (sp.act) {
+            act_bwd_kernel<<<(unsigned)((no + 255) / 256), 256, 0, s>>>(g, o, no);
+            NCK(cudaGetLastError());
+        }
+        ConvBwdW bw;
+        bw.in = conv_in(n, n->act, i, N);
+        bw.N = N;
+        bw.Ho = Ho;
+        bw.Wo = Wo;
+        bw.stride = sp.stride;
+        bw.cout = sp.cout;
+        bw.g = g;
+        bw.dw = n->grads + n->w_off[i];
+        bw.db = n->grads + n->b_off[i];
+        const int cin = sp.ca + sp.cb;
+        if (sp.cout % 8 == 0) conv_bwd_w_kernel<8><<<dim3(cin, sp.cout / 8), 256, 0, s>>>(bw);
+        else conv_bwd_w_kernel<2><<<dim3(cin, (sp.cout + 1) / 2), 256, 0, s>>>(bw);
+        NCK(cudaGetLastError());
+        if (sp.a == 0 && sp.b < 0) continue;  // the cost volume needs no gradient
+        ConvBwdData bd;
+        bd.N = N;
+        bd.cin = cin;
+        bd.Hin = bw.in.Hin;
+        bd.Win = bw.in.Win;
+        bd.Ho = Ho;
+        bd.Wo = Wo;
+        bd.stride = sp.stride;
+        bd.cout = sp.cout;
+        bd.w = n->wbf + n->w_off[i];
+        bd.g = g;
+        bd.din = n->din;
+        const int px = bd.Hin * bd.Win;
+        conv_bwd_data_kernel<32><<<dim3((px + 127) / 128, (cin + 31) / 32, N), 128, 0, s>>>(bd);
+        NCK(cudaGetLastError());
+        float *ga = sp.a > 0 ? n->gact + n->t_off[sp.a] : nullptr;
+        float *gb = sp.b >= 0 ? n->gact + n->t_off[sp.b] : nullptr;
+        const size_t tot = (ga ? (size_t)N * sp.ca * bw.in.Ha * bw.in.Wa : 0) + (gb ? (size_t)N * sp.cb * px : 0);
+        split_grad_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(n->din, N, sp.ca, sp.cb, sp.up, bd.Hin,
+                                                                         bd.Win, bw.in.Ha, bw.in.Wa, ga, gb);
+        NCK(cudaGetLastError());
+    }
+    NCK(cudaMemcpyAsync(n->h_loss, n->d_loss, sizeof(float), cudaMemcpyDeviceToHost, s));
+    NCK(cudaStreamSynchronize(s));
+    if (loss) *loss = *n->h_loss;
+    return PIV_OK;
+}
+
+int piv_net_adam_step(piv_net *n, float lr)
+{
+    if (!n || !(lr >= 0.f)) return PIV_ERR_ARG;
+    cudaSetDevice(n->device);
+    n->step += 1;
+    const float b1 = 0.9f, b2 = 0.999f;
+    const float c1 = (float)(1.0 / (1.0 - std::pow((double)b1, n->step)));
+    const float c2 = (float)(1.0 / (1.0 - std::pow((double)b2, n->step)));
+    adam_kernel<<<(unsigned)((n->n_params + 255) / 256), 256, 0, n->stream>>>(
+        n->params, n->grads, n->adam_m, n->adam_v, n->wbf, n->n_params, lr, b1, b2, 1e-8f, c1, c2);
+    NCK(cudaGetLastError());
+    return PIV_OK;
+}
+
+int piv_net_synchronize(piv_net *n)
+{
+    if (!n) return PIV_ERR_ARG;
+    cudaSetDevice(n->device);
+    NCK(cudaStreamSynchronize(n->stream));
+    return PIV_OK;
+}
+
+}  // extern "C"
