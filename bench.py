@@ -15,6 +15,9 @@ pair: 113,300 (412 x 275).
          (piv_queue_images), the pair, readback of the filtered grid-2 field
          (piv_field_async / piv_field_wait), every step, pipelined so that uploads and
          readbacks overlap the computation of the neighbouring pairs.
+  learned, learned_split_bf16  the learned form of the same pair (piv_run_pair_learned:
+         trained predictor instead of the grid-1 passes, grid-2 passes on FP32 SIMT or
+         split-BF16 tensor cores, judge with fallback), per-pair CUDA events.
   --impl reference  the reference's own engine (xcorr2d_multi + mhe_gpu, compiled for
          sm_100a from its sources) on the same pair through its public methods.
 
@@ -167,6 +170,45 @@ def cpu_baseline(P, f1, f2, rows):
                       f"({nvec} grid-2 vectors in {dt:.2f} s)"}
 
 
+def learned_form(P, e, ext, flush, args, s, path, plain_ms):
+    """The learned form of the same pair (piv_run_pair_learned): the predictor replaces the
+    grid-1 passes, grid 2 runs its 3 passes on `path`, and the judge (more than 5 % median
+    rejects, or more than 0.5 px RMS between the prediction and the grid-2 field) sends the
+    pair back to the plain method.  Timed per pair on the engine stream with CUDA events,
+    judge readback and any fallback included, L2 flushed before each pair."""
+    import torch
+
+    net = P.PredictorNet(weights=args.weights)
+    e.set_xcorr_path(1, path)
+    for _ in range(args.warmup):
+        e.run_pair_learned(net)
+    ms, fb, rej, rms = [], 0, [], []
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(ext)
+        r = e.run_pair_learned(net)
+        b.record(ext)
+        b.synchronize()
+        ms.append(a.elapsed_time(b))
+        fb += r["fell_back"]
+        rej.append(r["reject_frac"])
+        rms.append(r["rms_px"])
+    acc = accuracy(P, e, s)
+    e.set_xcorr_path(1, P.PIV_XCORR_SIMT)
+    net.close()
+    t = sum(ms) / len(ms)
+    return {"value": round(e.geom["Nt_vec"][1] / (t * 1e-3), 1), "unit": UNIT, "ms_per_step": round(t, 3),
+            "vs_plain": round(plain_ms / t, 3), "fallback_rate": fb / len(ms),
+            "judge": {"reject_frac": round(float(np.mean(rej)), 5), "rms_px": round(float(np.mean(rms)), 4),
+                      "limits": {"reject_frac": 0.05, "rms_px": 0.5}},
+            "accuracy": acc, "grid2_path": {P.PIV_XCORR_SIMT: "fp32 simt", P.PIV_XCORR_TC_SPLIT: "split-bf16 tcgen05",
+                                            P.PIV_XCORR_TC_BF16: "bf16 tcgen05"}[path],
+            "weights": str(Path(args.weights).relative_to(ROOT)) if Path(args.weights).is_relative_to(ROOT)
+            else str(args.weights)}
+
+
 def replicas():
     load_pkg()
     import piv_b200.replicas as R
@@ -268,6 +310,15 @@ def run_ours(args, rank, world, local):
         "e2e": e2e, "roofline": roofline, "gpu_launches": launches, "clocks": clk.summary(),
         "accuracy": acc,
     }
+    # the learned form beside the plain one (same engine, frames and flush)
+    plain_ms = total_s * 1e3 / args.steps
+    if Path(args.weights).exists():
+        e.set_device_images(d1.data_ptr(), d2.data_ptr())
+        s_true = workload_synth(P, seed=1 + rank)
+        out["learned"] = learned_form(P, e, ext, flush, args, s_true, P.PIV_XCORR_SIMT, plain_ms)
+        out["learned_split_bf16"] = learned_form(P, e, ext, flush, args, s_true, P.PIV_XCORR_TC_SPLIT, plain_ms)
+    else:
+        out["learned"] = {"unavailable": f"no predictor weights at {args.weights}"}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(P, f1, f2, args.cpu_rows)
     e.close()
@@ -321,6 +372,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-rows", type=int, default=1024, help="rows of the pair the CPU baseline processes")
+    ap.add_argument("--weights", default=str(PKG_DIR / "weights" / "predictor.bin"),
+                    help="learned-predictor weights (piv_xcorr2d_v1.0_b200/train_predictor.py)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":

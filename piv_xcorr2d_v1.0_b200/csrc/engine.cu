@@ -175,6 +175,7 @@ struct piv_engine {
     cudaGraphExec_t learned_exec = nullptr;
     const uint8_t *learned_in1 = nullptr, *learned_in2 = nullptr;
     const piv_net *learned_net = nullptr;
+    unsigned learned_gen = 0;
     float *d_pred2 = nullptr, *d_judge = nullptr, *h_judge = nullptr;
     std::string err;
     bool timing = false;
@@ -1048,7 +1049,8 @@ int piv_run_pair_learned(piv_engine *e, piv_net *n, float max_reject_frac, float
     }
     if ((rc = learned::net_reserve(n, 1, g1.gg.Ny_vec, g1.gg.Nx_vec))) return set_err(e, rc, "network buffers");
     if ((rc = learned::net_reserve_features(n, e->p.Nx, e->p.Ny))) return set_err(e, rc, "feature scratch");
-    if (!e->learned_exec || e->learned_in1 != e->d_in1 || e->learned_in2 != e->d_in2 || e->learned_net != n) {
+    if (!e->learned_exec || e->learned_in1 != e->d_in1 || e->learned_in2 != e->d_in2 || e->learned_net != n ||
+        e->learned_gen != learned::net_generation(n)) {
         if (e->learned_exec) cudaGraphExecDestroy(e->learned_exec);
         e->learned_exec = nullptr;
         cudaGraph_t g = nullptr;
@@ -1066,6 +1068,7 @@ int piv_run_pair_learned(piv_engine *e, piv_net *n, float max_reject_frac, float
         e->learned_in1 = e->d_in1;
         e->learned_in2 = e->d_in2;
         e->learned_net = n;
+        e->learned_gen = learned::net_generation(n);
     }
     CK(cudaGraphLaunch(e->learned_exec, e->stream));
     CK(cudaMemcpyAsync(e->h_judge, e->d_judge, 2 * sizeof(float), cudaMemcpyDeviceToHost, e->stream));
@@ -1312,10 +1315,12 @@ int piv_set_xcorr_path(piv_engine *e, int grid, int path)
     GridState &gs = e->grid[grid];
     if (path != PIV_XCORR_SIMT && !xcorr_tc_supported(gs.gg.ws_x, gs.gg.ws_y))
         return set_err(e, PIV_ERR_UNSUPPORTED, "window shape %dx%d has no tensor-core path", gs.gg.ws_x, gs.gg.ws_y);
-    if (gs.path != path && e->n_graphs) {
+    if (gs.path != path && (e->n_graphs || e->learned_exec)) {
         cudaStreamSynchronize(e->stream);
         for (int i = 0; i < e->n_graphs; ++i) cudaGraphExecDestroy(e->graphs[i].exec);
         e->n_graphs = 0;
+        if (e->learned_exec) cudaGraphExecDestroy(e->learned_exec);
+        e->learned_exec = nullptr;
     }
     gs.path = path;
     return PIV_OK;

@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -65,88 +66,116 @@ __device__ __forceinline__ float block_sum128(float v, float *red)
     return s;
 }
 
-// down[f][y][x] = mean of the 4x4 image block / 255; sums[f] += its total
+// down[f][y][x] = mean of the 4x4 image block / 255; sums[f] += its total.  A fixed
+// grid strides over the outputs so that the frame sums take one atomic add per block.
 __global__ void __launch_bounds__(128) down4_kernel(const uint8_t *f1, const uint8_t *f2, int pitch, int W4, int H4,
                                                     float *down, double *sums)
 {
     __shared__ float red[4];
     const int f = blockIdx.y;
     const uint8_t *src = f ? f2 : f1;
-    const int q = blockIdx.x * 128 + threadIdx.x;
-    float v = 0.f;
-    if (q < W4 * H4) {
+    const bool al4 = ((reinterpret_cast<uintptr_t>(src) | (uintptr_t)pitch) & 3) == 0;
+    float part = 0.f;
+    for (int q = blockIdx.x * 128 + threadIdx.x; q < W4 * H4; q += gridDim.x * 128) {
         const int y = q / W4, x = q - y * W4;
         const uint8_t *p = src + (size_t)(4 * y) * pitch + 4 * x;
         int s = 0;
+        if (al4) {
 #pragma unroll
-        for (int r = 0; r < 4; ++r)
+            for (int r = 0; r < 4; ++r) {
+                const uint32_t w = __ldg(reinterpret_cast<const uint32_t *>(p + (size_t)r * pitch));
+                s += (int)(w & 0xff) + (int)((w >> 8) & 0xff) + (int)((w >> 16) & 0xff) + (int)(w >> 24);
+            }
+        } else {
 #pragma unroll
-            for (int c = 0; c < 4; ++c) s += p[(size_t)r * pitch + c];
-        v = (float)s * (1.0f / (16.0f * 255.0f));
+            for (int r = 0; r < 4; ++r)
+#pragma unroll
+                for (int c = 0; c < 4; ++c) s += p[(size_t)r * pitch + c];
+        }
+        const float v = (float)s * (1.0f / (16.0f * 255.0f));
         down[(size_t)f * W4 * H4 + q] = v;
+        part += v;
     }
-    const float t = block_sum128(v, red);
+    const float t = block_sum128(part, red);
     if (threadIdx.x == 0) atomicAdd(sums + f, (double)t);
 }
 
-// One CTA per grid-1 vector.  Window of frame 1: WdxHd downsampled px around the window
-// centre; frame 2 region: the window grown by R on every side.  Outside the image the
-// mean-free frames are 0.
-__global__ void __launch_bounds__(128) cv_kernel(const float *down, const double *sums, int W4, int H4, GridGeom g,
-                                                 float *out)
+// Cost volume.  A CTA takes kCvVec consecutive vectors of kCvRows rows of the grid;
+// frame 1's windows and frame 2's region (the windows grown by R) are staged once in
+// shared memory, mean-free and zero outside the image (neighbouring windows overlap, so
+// the CTA's rows share most of it).  Thread (row, v, dy) computes the 9 shifts
+// (dy, 0..8) of its vector, sliding along each window row with the 9 frame-2 values in
+// registers; the dy = R thread also sums both windows' energies.
+constexpr int kCvVec = 16, kCvRows = 2;
+
+__host__ __device__ __forceinline__ int cv_centre(int i, int sp, int left, int ws) { return (i * sp - left + ws / 2 + kDown / 2) >> 2; }
+
+template <int WD>
+__global__ void __launch_bounds__(kCvVec *kShifts *kCvRows) cv_kernel(const float *down, const double *sums, int W4,
+                                                                      int H4, GridGeom g, int LW, int LHt, float *out)
 {
     extern __shared__ float sh[];
-    const int ix = blockIdx.x, iy = blockIdx.y;
-    const int Wd = g.ws_x / kDown, Hd = g.ws_y / kDown;
-    const int LW = Wd + 2 * kRadius, LH = Hd + 2 * kRadius;
-    float *s1 = sh, *s2 = sh + Wd * Hd;
-    __shared__ float red[4];
-    __shared__ float energy[2];
+    __shared__ float energy[kCvRows][kCvVec][2];
+    const int Wd = WD ? WD : g.ws_x / kDown, Hd = g.ws_y / kDown;
+    const int ix0 = blockIdx.x * kCvVec, iy0 = blockIdx.y * kCvRows;
+    const int nv = min(kCvVec, g.Nx_vec - ix0), nr = min(kCvRows, g.Ny_vec - iy0);
+    const int c0 = cv_centre(ix0, g.sp_x, g.Nx_left, g.ws_x), r0 = cv_centre(iy0, g.sp_y, g.Ny_left, g.ws_y);
+    const int xl = c0 - Wd / 2 - kRadius, yl = r0 - Hd / 2 - kRadius;
+    const int L1W = LW - 2 * kRadius, L1H = LHt - 2 * kRadius;
+    float *s2 = sh, *s1 = sh + LHt * LW;
     const float m1 = (float)(sums[0] / ((double)W4 * H4)), m2 = (float)(sums[1] / ((double)W4 * H4));
-    const int cx = ix * g.sp_x - g.Nx_left + g.ws_x / 2, cy = iy * g.sp_y - g.Ny_left + g.ws_y / 2;
-    // nearest block boundary to the centre, in downsampled px
-    const int dcx = (cx + kDown / 2) >> 2, dcy = (cy + kDown / 2) >> 2;
-    const int x0 = dcx - Wd / 2, y0 = dcy - Hd / 2;
     const float *d1 = down, *d2 = down + (size_t)W4 * H4;
-    for (int e = threadIdx.x; e < Wd * Hd; e += 128) {
-        const int r = e / Wd, c = e - r * Wd;
-        const int y = y0 + r, x = x0 + c;
-        s1[e] = (x >= 0 && x < W4 && y >= 0 && y < H4) ? d1[(size_t)y * W4 + x] - m1 : 0.f;
-    }
-    for (int e = threadIdx.x; e < LW * LH; e += 128) {
+    for (int e = threadIdx.x; e < LHt * LW; e += blockDim.x) {
         const int r = e / LW, c = e - r * LW;
-        const int y = y0 - kRadius + r, x = x0 - kRadius + c;
-        s2[e] = (x >= 0 && x < W4 && y >= 0 && y < H4) ? d2[(size_t)y * W4 + x] - m2 : 0.f;
+        const int y = yl + r, x = xl + c;
+        s2[e] = (x >= 0 && x < W4 && y >= 0 && y < H4) ? __ldg(d2 + (size_t)y * W4 + x) - m2 : 0.f;
+    }
+    for (int e = threadIdx.x; e < L1H * L1W; e += blockDim.x) {
+        const int r = e / L1W, c = e - r * L1W;
+        const int y = yl + kRadius + r, x = xl + kRadius + c;
+        s1[e] = (x >= 0 && x < W4 && y >= 0 && y < H4) ? __ldg(d1 + (size_t)y * W4 + x) - m1 : 0.f;
     }
     __syncthreads();
-    // window energies (frame 2 at zero shift)
+    const int row = threadIdx.x / (kCvVec * kShifts);
+    const int rem = threadIdx.x - row * (kCvVec * kShifts);
+    const int v = rem / kShifts, dy = rem - v * kShifts;
+    const bool live = v < nv && row < nr;
+    float acc[kShifts];
+#pragma unroll
+    for (int k = 0; k < kShifts; ++k) acc[k] = 0.f;
     float e1 = 0.f, e2 = 0.f;
-    for (int e = threadIdx.x; e < Wd * Hd; e += 128) {
-        const int r = e / Wd, c = e - r * Wd;
-        const float a = s1[e], b = s2[(r + kRadius) * LW + c + kRadius];
-        e1 += a * a;
-        e2 += b * b;
-    }
-    const float t1 = block_sum128(e1, red);
-    __syncthreads();
-    const float t2 = block_sum128(e2, red);
-    if (threadIdx.x == 0) {
-        energy[0] = t1;
-        energy[1] = t2;
-    }
-    __syncthreads();
-    const int t = threadIdx.x;
-    if (t < kInChannels) {
-        const int dy = t / kShifts, dx = t - dy * kShifts;  // shift + R
-        float acc = 0.f;
+    if (live) {
+        const int offx = cv_centre(ix0 + v, g.sp_x, g.Nx_left, g.ws_x) - c0;
+        const int offy = cv_centre(iy0 + row, g.sp_y, g.Ny_left, g.ws_y) - r0;
         for (int r = 0; r < Hd; ++r) {
-            const float *a = s1 + r * Wd, *b = s2 + (r + dy) * LW + dx;
-            for (int c = 0; c < Wd; ++c) acc = fmaf(a[c], b[c], acc);
+            const float *a = s1 + (offy + r) * L1W + offx, *b = s2 + (offy + r + dy) * LW + offx;
+            float win[kShifts];
+#pragma unroll
+            for (int q = 0; q < kShifts - 1; ++q) win[q] = b[q];
+#pragma unroll(WD ? WD : 1)
+            for (int c = 0; c < Wd; ++c) {
+                win[kShifts - 1] = b[c + kShifts - 1];
+                const float av = a[c];
+#pragma unroll
+                for (int k = 0; k < kShifts; ++k) acc[k] = fmaf(av, win[k], acc[k]);
+                e1 = fmaf(av, av, e1);
+                e2 = fmaf(win[kRadius], win[kRadius], e2);
+#pragma unroll
+                for (int q = 0; q < kShifts - 1; ++q) win[q] = win[q + 1];
+            }
         }
-        const float den = energy[0] * energy[1];
-        const float v = den > 0.f ? acc * rsqrtf(den) : 0.f;
-        out[((size_t)t * g.Ny_vec + iy) * g.Nx_vec + ix] = v;
+        if (dy == kRadius) {
+            energy[row][v][0] = e1;
+            energy[row][v][1] = e2;
+        }
     }
+    __syncthreads();
+    if (!live) return;
+    const float den = energy[row][v][0] * energy[row][v][1];
+    const float sc = den > 0.f ? rsqrtf(den) : 0.f;
+    const size_t plane = (size_t)g.Ny_vec * g.Nx_vec, o = (size_t)(iy0 + row) * g.Nx_vec + ix0 + v;
+#pragma unroll
+    for (int k = 0; k < kShifts; ++k) out[(size_t)(dy * kShifts + k) * plane + o] = acc[k] * sc;
 }
 
 size_t feature_scratch_floats(int Nx, int Ny) { return (size_t)2 * (Nx / kDown) * (Ny / kDown); }
@@ -157,12 +186,30 @@ cudaError_t launch_features(const FeatArgs &a, cudaStream_t s)
     if (W4 < 1 || H4 < 1 || a.g.ws_x < 2 * kDown || a.g.ws_y < 2 * kDown) return cudaErrorInvalidValue;
     cudaError_t e = cudaMemsetAsync(a.sums, 0, 2 * sizeof(double), s);
     if (e != cudaSuccess) return e;
-    down4_kernel<<<dim3((W4 * H4 + 127) / 128, 2), 128, 0, s>>>(a.f1, a.f2, a.pitch, W4, H4, a.down, a.sums);
+    const int blocks = std::min((W4 * H4 + 127) / 128, 4 * 148);
+    down4_kernel<<<dim3(blocks, 2), 128, 0, s>>>(a.f1, a.f2, a.pitch, W4, H4, a.down, a.sums);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     const int Wd = a.g.ws_x / kDown, Hd = a.g.ws_y / kDown;
-    const size_t smem = sizeof(float) * ((size_t)Wd * Hd + (size_t)(Wd + 2 * kRadius) * (Hd + 2 * kRadius));
+    // widest frame-2 region of a CTA: the spread of its vector centres plus a window and 2R
+    int spread = 0;
+    for (int ix0 = 0; ix0 < a.g.Nx_vec; ix0 += kCvVec) {
+        const int last = std::min(ix0 + kCvVec, a.g.Nx_vec) - 1;
+        spread = std::max(spread, cv_centre(last, a.g.sp_x, a.g.Nx_left, a.g.ws_x) -
+                                      cv_centre(ix0, a.g.sp_x, a.g.Nx_left, a.g.ws_x));
+    }
+    int spread_y = 0;
+    for (int iy0 = 0; iy0 < a.g.Ny_vec; iy0 += kCvRows) {
+        const int last = std::min(iy0 + kCvRows, a.g.Ny_vec) - 1;
+        spread_y = std::max(spread_y, cv_centre(last, a.g.sp_y, a.g.Ny_left, a.g.ws_y) -
+                                          cv_centre(iy0, a.g.sp_y, a.g.Ny_left, a.g.ws_y));
+    }
+    const int LW = spread + Wd + 2 * kRadius, LHt = spread_y + Hd + 2 * kRadius;
+    const size_t smem = sizeof(float) * ((size_t)LHt * LW + (size_t)(LHt - 2 * kRadius) * (LW - 2 * kRadius));
     if (smem > 48 * 1024) return cudaErrorInvalidValue;
-    cv_kernel<<<dim3(a.g.Nx_vec, a.g.Ny_vec), 128, smem, s>>>(a.down, a.sums, W4, H4, a.g, a.out);
+    const dim3 grid((a.g.Nx_vec + kCvVec - 1) / kCvVec, (a.g.Ny_vec + kCvRows - 1) / kCvRows);
+    const int nt = kCvVec * kShifts * kCvRows;
+    if (Wd == 16) cv_kernel<16><<<grid, nt, smem, s>>>(a.down, a.sums, W4, H4, a.g, LW, LHt, a.out);
+    else cv_kernel<0><<<grid, nt, smem, s>>>(a.down, a.sums, W4, H4, a.g, LW, LHt, a.out);
     return cudaGetLastError();
 }
 
@@ -217,52 +264,82 @@ __device__ __forceinline__ void conv_gather(const ConvIn &c, int n, int ci, cons
     }
 }
 
-// Thread per output pixel, COB output channels per CTA; weights staged through shared
-// memory CIC input channels at a time, laid [ci][tap][co] so every FMA reads a broadcast.
-template <int COB>
-__global__ void __launch_bounds__(128) conv_fwd_kernel(const ConvFwd c)
+// Forward convolution as a split-K implicit GEMM: a CTA computes 32 output pixels
+// (lane = pixel) x COT output channels; its 8 warps take the input channels in turn, two
+// per iteration (both channels' loads in flight before their FMAs), each staging those
+// channels' COT x 9 weights in its own shared slice (FMAs read broadcasts); the partial
+// sums are reduced through shared memory, which the weight slices alias.  The small
+// vector grids of the coarse levels still fill the GPU this way.
+constexpr int kConvWarps = 8;
+
+template <int COT>
+constexpr size_t conv_fwd_smem()
 {
-    constexpr int CIC = 8;
-    __shared__ __align__(16) float ws[CIC][9][COB];
-    const int n = blockIdx.z, co0 = blockIdx.y * COB;
-    const int p = blockIdx.x * 128 + threadIdx.x;
-    const bool live = p < c.Ho * c.Wo;
+    const size_t w = (size_t)kConvWarps * 2 * 9 * COT, r = (size_t)kConvWarps * COT * 33;
+    return (w > r ? w : r) * sizeof(float);
+}
+
+template <int COT>
+__global__ void __launch_bounds__(256) conv_fwd_kernel(const ConvFwd c)
+{
+    constexpr int NW = kConvWarps;
+    extern __shared__ __align__(16) float csm[];
+    float(*wsm)[2][9][COT] = reinterpret_cast<float(*)[2][9][COT]>(csm);  // [warp][buffer][tap][co]
+    float(*red)[COT][33] = reinterpret_cast<float(*)[COT][33]>(csm);      // [warp][co][pixel]
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int n = blockIdx.z, co0 = blockIdx.y * COT;
+    const int HWo = c.Ho * c.Wo;
+    const int p = blockIdx.x * 32 + lane;
+    const bool live = p < HWo;
     const int oy = live ? p / c.Wo : 0, ox = live ? p - oy * c.Wo : 0;
     const int cin = c.in.ca + c.in.cb;
     int oa[9], ob[9];
     conv_taps(c.in, oy, ox, c.stride, live, oa, ob);
-    float acc[COB];
+    float acc[COT];
 #pragma unroll
-    for (int k = 0; k < COB; ++k) acc[k] = 0.f;
-    for (int ci0 = 0; ci0 < cin; ci0 += CIC) {
-        __syncthreads();
-        for (int e = threadIdx.x; e < CIC * 9 * COB; e += 128) {
-            const int co = e % COB, r = e / COB, tap = r % 9, ci = r / 9;
-            float wv = 0.f;
-            if (ci0 + ci < cin && co0 + co < c.cout)
-                wv = __bfloat162float(c.w[((size_t)(co0 + co) * cin + ci0 + ci) * 9 + tap]);
-            ws[ci][tap][co] = wv;
-        }
-        __syncthreads();
-        const int nci = min(CIC, cin - ci0);
+    for (int k = 0; k < COT; ++k) acc[k] = 0.f;
 #pragma unroll 1
-        for (int ci = 0; ci < nci; ++ci) {
-            float x[9];
-            conv_gather(c.in, n, ci0 + ci, oa, ob, x);
-#pragma unroll
-            for (int t = 0; t < 9; ++t)
-#pragma unroll
-                for (int k = 0; k < COB; ++k) acc[k] = fmaf(ws[ci][t][k], x[t], acc[k]);
+    for (int ci = warp; ci < cin; ci += 2 * NW) {
+        const int cj = ci + NW;
+        const bool two = cj < cin;
+        for (int e = lane; e < 9 * COT; e += 32) {
+            const int co = e / 9, tap = e - co * 9;
+            const bool ok = co0 + co < c.cout;
+            const size_t base = (size_t)(co0 + co) * cin * 9 + tap;
+            wsm[warp][0][tap][co] = ok ? __bfloat162float(c.w[base + (size_t)ci * 9]) : 0.f;
+            wsm[warp][1][tap][co] = ok && two ? __bfloat162float(c.w[base + (size_t)cj * 9]) : 0.f;
         }
-    }
-    if (!live) return;
+        __syncwarp();
+        float x0[9], x1[9];
+        conv_gather(c.in, n, ci, oa, ob, x0);
+        if (two) conv_gather(c.in, n, cj, oa, ob, x1);
+        else {
 #pragma unroll
-    for (int k = 0; k < COB; ++k) {
-        const int co = co0 + k;
-        if (co >= c.cout) break;
-        float v = acc[k] + c.bias[co];
+            for (int t = 0; t < 9; ++t) x1[t] = 0.f;
+        }
+#pragma unroll
+        for (int t = 0; t < 9; ++t)
+#pragma unroll
+            for (int k = 0; k < COT; ++k) acc[k] = fmaf(wsm[warp][0][t][k], x0[t], acc[k]);
+#pragma unroll
+        for (int t = 0; t < 9; ++t)
+#pragma unroll
+            for (int k = 0; k < COT; ++k) acc[k] = fmaf(wsm[warp][1][t][k], x1[t], acc[k]);
+        __syncwarp();
+    }
+    __syncthreads();  // every warp is done with its weight slices: the reduction reuses them
+#pragma unroll
+    for (int k = 0; k < COT; ++k) red[warp][k][lane] = acc[k];
+    __syncthreads();
+    for (int e = threadIdx.x; e < 32 * COT; e += 256) {
+        const int k = e >> 5, l = e & 31;
+        const int pp = blockIdx.x * 32 + l, co = co0 + k;
+        if (pp >= HWo || co >= c.cout) continue;
+        float v = c.bias[co];
+#pragma unroll
+        for (int w = 0; w < NW; ++w) v += red[w][k][l];
         if (c.act) v = v > 0.f ? v : kSlope * v;
-        c.out[((size_t)n * c.cout + co) * c.Ho * c.Wo + p] = v;
+        c.out[((size_t)n * c.cout + co) * HWo + pp] = v;
     }
 }
 
@@ -509,34 +586,34 @@ cudaError_t launch_field_from_net(const float *out, int Nt, float *fx, float *fy
     return cudaGetLastError();
 }
 
-__global__ void __launch_bounds__(1024) judge_kernel(const float *px, const float *py, const float *fx,
-                                                     const float *fy, int Nt, const int *list_n, float *judge)
+__global__ void __launch_bounds__(256) judge_kernel(const float *px, const float *py, const float *fx,
+                                                    const float *fy, int Nt, const int *list_n, float *judge)
 {
-    __shared__ float red[32];
+    __shared__ float red[8];
     float s = 0.f;
-    for (int i = threadIdx.x; i < Nt; i += 1024) {
+    for (int i = blockIdx.x * 256 + threadIdx.x; i < Nt; i += gridDim.x * 256) {
         const float dx = px[i] - fx[i], dy = py[i] - fy[i];
-        s += dx * dx + dy * dy;
+        s = fmaf(dx, dx, fmaf(dy, dy, s));
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
     __syncthreads();
-    if (threadIdx.x < 32) {
-        float v = red[threadIdx.x];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-        if (threadIdx.x == 0) {
-            judge[0] = v;
-            judge[1] = (float)*list_n;
-        }
+    if (threadIdx.x == 0) {
+        float v = 0.f;
+        for (int w = 0; w < 8; ++w) v += red[w];
+        atomicAdd(judge, v);
+        if (blockIdx.x == 0) judge[1] = (float)*list_n;
     }
 }
 
 cudaError_t launch_judge(const float *px, const float *py, const float *fx, const float *fy, int Nt,
                          const int *list_n, float *judge, cudaStream_t s)
 {
-    judge_kernel<<<1, 1024, 0, s>>>(px, py, fx, fy, Nt, list_n, judge);
+    cudaError_t e = cudaMemsetAsync(judge, 0, sizeof(float), s);
+    if (e != cudaSuccess) return e;
+    const int blocks = std::max(1, std::min((Nt + 255) / 256, 148));
+    judge_kernel<<<blocks, 256, 0, s>>>(px, py, fx, fy, Nt, list_n, judge);
     return cudaGetLastError();
 }
 
@@ -566,9 +643,18 @@ struct piv_net {
     size_t fcap = 0;
     cudaStream_t stream = nullptr;
     std::string err;
+    // drawn from a process-wide counter at creation and whenever a buffer a captured graph
+    // may hold is reallocated or re-laid-out, so (net, generation) never repeats
+    unsigned generation = 0;
 };
 
 namespace {
+
+unsigned next_generation()
+{
+    static std::atomic<unsigned> g{0};
+    return ++g;
+}
 
 int net_err(piv_net *n, int code, const char *msg)
 {
@@ -643,9 +729,9 @@ cudaError_t forward_layers(piv_net *n, float *act, int N, cudaStream_t s)
         c.act = sp.act;
         const int px = c.Ho * c.Wo;
         if (sp.cout % 32 == 0) {
-            conv_fwd_kernel<32><<<dim3((px + 127) / 128, sp.cout / 32, N), 128, 0, s>>>(c);
+            conv_fwd_kernel<32><<<dim3((px + 31) / 32, sp.cout / 32, N), 256, conv_fwd_smem<32>(), s>>>(c);
         } else {
-            conv_fwd_kernel<2><<<dim3((px + 127) / 128, (sp.cout + 1) / 2, N), 128, 0, s>>>(c);
+            conv_fwd_kernel<2><<<dim3((px + 31) / 32, (sp.cout + 1) / 2, N), 256, conv_fwd_smem<2>(), s>>>(c);
         }
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
@@ -663,6 +749,7 @@ int net_reserve(piv_net *n, int N, int H, int W)
     if (!n || N < 1 || H < 1 || W < 1) return PIV_ERR_ARG;
     if (n->act && n->aN == N && n->aH == H && n->aW == W) return PIV_OK;
     cudaSetDevice(n->device);
+    n->generation = next_generation();
     const size_t old_act = n->act ? n->act_floats : 0, old_din = n->act ? n->din_floats : 0;
     layout(n, N, H, W);
     if (n->act_floats > old_act || n->din_floats > old_din || !n->act) {
@@ -706,6 +793,7 @@ int net_reserve_features(piv_net *n, int Nx, int Ny)
     const size_t need = feature_scratch_floats(Nx, Ny);
     if (n->fdown && n->fcap >= need) return PIV_OK;
     cudaSetDevice(n->device);
+    n->generation = next_generation();
     cudaFree(n->fdown);
     n->fdown = nullptr;
     NCK(cudaMalloc(&n->fdown, need * sizeof(float)));
@@ -714,6 +802,7 @@ int net_reserve_features(piv_net *n, int Nx, int Ny)
     return PIV_OK;
 }
 
+unsigned net_generation(const piv_net *n) { return n->generation; }
 float *net_feature_down(piv_net *n) { return n->fdown; }
 double *net_feature_sums(piv_net *n) { return n->fsums; }
 
@@ -730,6 +819,7 @@ int piv_net_create(uint64_t seed, piv_net **out)
     if (!out) return PIV_ERR_ARG;
     *out = nullptr;
     piv_net *n = new piv_net;
+    n->generation = next_generation();
     cudaGetDevice(&n->device);
     size_t off = 0;
     for (int i = 0; i < kLayers; ++i) {

@@ -53,6 +53,9 @@ cudaError_t launch_field_from_net(const float *out, int Nt, float *fx, float *fy
 // median test's rejects)
 cudaError_t launch_judge(const float *px, const float *py, const float *fx, const float *fy, int Nt,
                          const int *list_n, float *judge, cudaStream_t s);
+// changes whenever net_reserve / net_reserve_features move or re-lay-out a buffer: a
+// graph captured with the net's buffers is stale once it differs
+unsigned net_generation(const piv_net *n);
 // feature scratch owned by the net (sized for the largest frame seen)
 int net_reserve_features(piv_net *n, int Nx, int Ny);
 float *net_feature_down(piv_net *n);
