@@ -362,6 +362,29 @@ int piv_synth_field(const piv_synth_params *s, const float *x, const float *y, i
  * d_scratch: 2*Nx*Ny floats (device); stream: cudaStream_t or NULL.  Asynchronous. */
 int piv_synth_pair_device(const piv_synth_params *s, uint8_t *d_f1, uint8_t *d_f2, float *d_scratch, void *stream);
 
+/* ---- batches of uneven pairs (no reference counterpart) ----------------------------
+ * n pairs of any sizes and window shapes (params[i]; every pair must have the same
+ * Npass1 and Npass2), one engine each.  piv_batch_run runs every pair's pass loop as one
+ * captured graph: per pass, the pairs' deformations and validations on parallel
+ * branches and ONE persistent correlation launch per (grid, window shape, top-K width)
+ * group over all pairs in it, instead of one launch per pair.  The first run autotunes
+ * each group's tile variant on the batch's data.  Results are bit-identical to
+ * piv_run_pair on each engine.  Frames: set on each engine (piv_batch_engine +
+ * piv_set_images / piv_set_device_images / piv_host_images) before piv_batch_run; read
+ * fields from the engines after piv_batch_synchronize.  Asynchronous. */
+typedef struct piv_batch piv_batch;
+int piv_batch_create(const piv_params *params, int n, piv_batch **out);
+int piv_batch_destroy(piv_batch *b);
+const char *piv_batch_last_error(const piv_batch *b);
+int piv_batch_engine(piv_batch *b, int i, piv_engine **e);
+int piv_batch_run(piv_batch *b);
+int piv_batch_synchronize(piv_batch *b);
+int piv_batch_stream(const piv_batch *b, void **stream);
+/* The correlation groups (up to max): window shape, grid (0/1), deformed pass or not,
+ * pairs in the group, chosen tile variant and its windows per CTA; *n_groups = count. */
+int piv_batch_groups(const piv_batch *b, int max, int *wsx, int *wsy, int *grid, int *deformed, int *pairs,
+                     int *variant, int *windows_per_cta, int *n_groups);
+
 /* ---- learned grid-1 predictor (no reference counterpart) --------------------------
  * Replaces the plain grid-1 passes (X/main.cpp:290-300 driving Calc_cc_map_p1 and
  * MedianFilter_Smoothing_p1) as the deformation predictor of the grid-2 passes.

@@ -155,6 +155,14 @@ EXPORTS = {
     "piv_synth_pair": (C.c_int, [C.POINTER(PivSynthParams), _U8, _U8]),
     "piv_synth_field": (C.c_int, [C.POINTER(PivSynthParams), _F, _F, C.c_int, _F, _F]),
     "piv_synth_pair_device": (C.c_int, [C.POINTER(PivSynthParams), _P, _P, _P, _P]),
+    "piv_batch_create": (C.c_int, [C.POINTER(PivParams), C.c_int, C.POINTER(_P)]),
+    "piv_batch_destroy": (C.c_int, [_P]),
+    "piv_batch_last_error": (C.c_char_p, [_P]),
+    "piv_batch_engine": (C.c_int, [_P, C.c_int, C.POINTER(_P)]),
+    "piv_batch_run": (C.c_int, [_P]),
+    "piv_batch_synchronize": (C.c_int, [_P]),
+    "piv_batch_stream": (C.c_int, [_P, C.POINTER(_P)]),
+    "piv_batch_groups": (C.c_int, [_P, C.c_int] + [C.POINTER(C.c_int)] * 8),
     "piv_net_create": (C.c_int, [C.c_uint64, C.POINTER(_P)]),
     "piv_net_destroy": (C.c_int, [_P]),
     "piv_net_last_error": (C.c_char_p, [_P]),
@@ -320,6 +328,69 @@ def net_layout():
     return out
 
 
+class Batch:
+    """Pairs of uneven size and window shape run together (piv_batch_*): one persistent
+    correlation launch per pass and window shape, the pass loop as one CUDA graph.
+    `engines[i]` is pair i's engine (set its frames, read its fields)."""
+
+    def __init__(self, params_list):
+        n = len(params_list)
+        arr = (PivParams * n)(*params_list)
+        h = C.c_void_p()
+        rc = lib().piv_batch_create(arr, n, C.byref(h))
+        if rc != PIV_OK:
+            raise PivError(rc, "piv_batch_create failed")
+        self.h = h
+        self.engines = []
+        for i in range(n):
+            e = C.c_void_p()
+            self._ck(lib().piv_batch_engine(self.h, i, C.byref(e)))
+            self.engines.append(Engine._borrowed(e, params_list[i]))
+
+    def _ck(self, rc):
+        if rc != PIV_OK:
+            raise PivError(rc, lib().piv_batch_last_error(self.h).decode())
+        return rc
+
+    def run(self):
+        self._ck(lib().piv_batch_run(self.h))
+
+    def synchronize(self):
+        self._ck(lib().piv_batch_synchronize(self.h))
+
+    def stream(self) -> int:
+        s = C.c_void_p()
+        self._ck(lib().piv_batch_stream(self.h, C.byref(s)))
+        return s.value or 0
+
+    def groups(self):
+        n = C.c_int()
+        self._ck(lib().piv_batch_groups(self.h, 0, *([None] * 7), C.byref(n)))
+        cols = [(C.c_int * max(n.value, 1))() for _ in range(7)]
+        self._ck(lib().piv_batch_groups(self.h, n.value, *cols, C.byref(n)))
+        keys = ("wsx", "wsy", "grid", "deformed", "pairs", "variant", "windows_per_cta")
+        return [{k: cols[j][i] for j, k in enumerate(keys)} for i in range(n.value)]
+
+    def close(self):
+        if getattr(self, "h", None):
+            for e in self.engines:
+                e.h = None
+            lib().piv_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+
 class PredictorNet:
     """The learned grid-1 predictor (piv_net_*): a 4-level U-Net on the cost volume of the
     4x-downsampled frames, BF16 weights, hand-written training and inference kernels."""
@@ -409,10 +480,23 @@ class Engine:
         lib().piv_get_geometry(self.h, C.byref(g))
         self.geom = g.to_dict()
 
+    @classmethod
+    def _borrowed(cls, handle, params: PivParams):
+        """An engine owned by someone else (a batch): no piv_destroy on close."""
+        e = cls.__new__(cls)
+        e.p = params
+        e.h = handle
+        e._owner = False
+        g = PivGeometry()
+        lib().piv_get_geometry(e.h, C.byref(g))
+        e.geom = g.to_dict()
+        return e
+
     # -- lifetime --
     def close(self):
         if getattr(self, "h", None):
-            lib().piv_destroy(self.h)
+            if getattr(self, "_owner", True):
+                lib().piv_destroy(self.h)
             self.h = None
 
     def __del__(self):

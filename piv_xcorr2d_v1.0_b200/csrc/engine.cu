@@ -329,6 +329,31 @@ int do_prep(piv_engine *e)
     return PIV_OK;
 }
 
+// Arguments of grid k's correlation launch over all its windows.
+XcorrArgs xcorr_args(piv_engine *e, int k)
+{
+    GridState &gs = e->grid[k];
+    XcorrArgs a;
+    a.g = gs.gg;
+    a.f1 = frame_of(e, e->d_f1);
+    a.f2 = frame_of(e, e->d_f2);
+    a.def = gs.def;
+    a.def_pitch = gs.def_pitch;
+    a.pred_x = gs.fx;
+    a.pred_y = gs.fy;
+    a.cdx = gs.cdx;
+    a.cdy = gs.cdy;
+    a.cvalid = gs.cv;
+    a.count = gs.count;
+    a.pidx = gs.pidx;
+    a.pval = gs.pval;
+    a.cc_dump = nullptr;
+    a.status = e->d_status;
+    a.w_first = 0;
+    a.w_end = gs.gg.Nt_vec;
+    return a;
+}
+
 int do_xcorr(piv_engine *e, int k, bool deformed, int first, int end, float *dump)
 {
     GridState &gs = e->grid[k];
@@ -1498,6 +1523,394 @@ int piv_mhe_destroy(piv_mhe *m)
     if (!m) return PIV_ERR_ARG;
     cudaFree(m->d_levels);
     delete m;
+    return PIV_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------------------
+// Batches of pairs of uneven size and window shape (piv_batch_*; no reference
+// counterpart).  One engine per pair holds its frames, geometry and fields; the batch
+// runs their pass loop together: per pass, the pairs' deformations on parallel graph
+// branches, then ONE persistent correlation launch per (grid, window shape, top-K width)
+// over all pairs that share it, then the pairs' validations on parallel branches.  The
+// whole loop is one captured CUDA graph.  The first run autotunes the tile variant of
+// every shape group on the batch's own data.
+// ------------------------------------------------------------------------------
+struct piv_batch {
+    int n = 0, device = 0;
+    std::vector<piv_engine *> eng;
+    cudaStream_t stream = nullptr;
+    std::vector<cudaStream_t> workers;
+    std::vector<cudaEvent_t> ev_join;
+    cudaEvent_t ev_fork = nullptr;
+    struct Group {
+        int k = 0;
+        bool deformed = false;
+        int wsx = 0, wsy = 0, K = 4;
+        std::vector<int> pairs;
+        XcorrArgs *d_args = nullptr;
+        int *d_first[2] = {};
+        int items[2] = {};
+        int n_variants = 0, variant = 0;
+        float tuned_ms[2] = {};
+    };
+    std::vector<Group> groups;
+    bool tuned = false;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<const uint8_t *> graph_in;
+    std::string err;
+};
+
+namespace {
+
+int batch_err(piv_batch *b, int code, const char *fmt, ...)
+{
+    if (b) {
+        char buf[512];
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(buf, sizeof(buf), fmt, ap);
+        va_end(ap);
+        b->err = buf;
+    }
+    return code;
+}
+
+#define BCK(call)                                                                                              \
+    do {                                                                                                       \
+        cudaError_t _e = (call);                                                                               \
+        if (_e != cudaSuccess) return batch_err(b, PIV_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(_e));      \
+    } while (0)
+
+void batch_free(piv_batch *b)
+{
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    for (auto &g : b->groups) {
+        cudaFree(g.d_args);
+        cudaFree(g.d_first[0]);
+        cudaFree(g.d_first[1]);
+    }
+    for (cudaStream_t s : b->workers) cudaStreamDestroy(s);
+    for (cudaEvent_t ev : b->ev_join) cudaEventDestroy(ev);
+    if (b->ev_fork) cudaEventDestroy(b->ev_fork);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    for (piv_engine *e : b->eng)
+        if (e) piv_destroy(e);
+}
+
+// the groups' argument tables (the engines' buffers are fixed after creation)
+int batch_build_groups(piv_batch *b)
+{
+    for (int k = 0; k < 2; ++k)
+        for (int d = 0; d < 2; ++d) {
+            for (int i = 0; i < b->n; ++i) {
+                piv_engine *e = b->eng[i];
+                const int np = k ? e->p.Npass2 : e->p.Npass1;
+                if (np == 0) continue;
+                const bool deformed = d == 1;
+                if (!deformed && k == 1) continue;   // grid 2 passes are all deformed
+                if (deformed && k == 0 && np < 2) continue;
+                const GridState &gs = e->grid[k];
+                const int K = gs.gg.Nps <= 4 ? 4 : 8;
+                piv_batch::Group *grp = nullptr;
+                for (auto &g : b->groups)
+                    if (g.k == k && g.deformed == deformed && g.wsx == gs.gg.ws_x && g.wsy == gs.gg.ws_y && g.K == K)
+                        grp = &g;
+                if (!grp) {
+                    b->groups.emplace_back();
+                    grp = &b->groups.back();
+                    grp->k = k;
+                    grp->deformed = deformed;
+                    grp->wsx = gs.gg.ws_x;
+                    grp->wsy = gs.gg.ws_y;
+                    grp->K = K;
+                    grp->n_variants = std::min(2, xcorr_batch_variants(gs.gg.ws_x, gs.gg.ws_y));
+                }
+                grp->pairs.push_back(i);
+            }
+        }
+    for (auto &g : b->groups) {
+        if (g.n_variants < 1) return batch_err(b, PIV_ERR_UNSUPPORTED, "window shape %dx%d has no batch launch", g.wsx, g.wsy);
+        std::vector<XcorrArgs> args;
+        for (int i : g.pairs) args.push_back(xcorr_args(b->eng[i], g.k));
+        BCK(cudaMalloc(&g.d_args, args.size() * sizeof(XcorrArgs)));
+        BCK(cudaMemcpy(g.d_args, args.data(), args.size() * sizeof(XcorrArgs), cudaMemcpyHostToDevice));
+        for (int v = 0; v < g.n_variants; ++v) {
+            const int B = xcorr_batch_windows_per_cta(g.wsx, g.wsy, v);
+            std::vector<int> first(1, 0);
+            for (const XcorrArgs &a : args) first.push_back(first.back() + (a.w_end - a.w_first + B - 1) / B);
+            g.items[v] = first.back();
+            BCK(cudaMalloc(&g.d_first[v], first.size() * sizeof(int)));
+            BCK(cudaMemcpy(g.d_first[v], first.data(), first.size() * sizeof(int), cudaMemcpyHostToDevice));
+        }
+    }
+    return PIV_OK;
+}
+
+int batch_launch_group(piv_batch *b, const piv_batch::Group &g, int variant)
+{
+    XcorrBatch xb;
+    xb.pairs = g.d_args;
+    xb.first = g.d_first[variant];
+    xb.n = (int)g.pairs.size();
+    xb.items = g.items[variant];
+    const char *why = nullptr;
+    cudaError_t c = launch_xcorr_batch(g.wsx, g.wsy, variant, xb, g.deformed, g.K, b->stream, &why);
+    if (c != cudaSuccess) return batch_err(b, PIV_ERR_CUDA, "batch correlation: %s", why ? why : cudaGetErrorString(c));
+    return PIV_OK;
+}
+
+// The pass loop of every pair, queued on the batch stream with per-pair stages on the
+// worker streams (fork / join through events; inside a capture these become parallel
+// graph branches).
+int batch_enqueue(piv_batch *b)
+{
+    const int W = (int)b->workers.size();
+    std::vector<cudaStream_t> own(b->n);
+    for (int i = 0; i < b->n; ++i) {
+        own[i] = b->eng[i]->stream;
+        b->eng[i]->stream = b->workers[i % W];
+    }
+    auto restore = [&]() {
+        for (int i = 0; i < b->n; ++i) b->eng[i]->stream = own[i];
+    };
+    auto fork = [&]() -> int {
+        BCK(cudaEventRecord(b->ev_fork, b->stream));
+        for (cudaStream_t w : b->workers) BCK(cudaStreamWaitEvent(w, b->ev_fork, 0));
+        return PIV_OK;
+    };
+    auto join = [&]() -> int {
+        for (int w = 0; w < W; ++w) {
+            BCK(cudaEventRecord(b->ev_join[w], b->workers[w]));
+            BCK(cudaStreamWaitEvent(b->stream, b->ev_join[w], 0));
+        }
+        return PIV_OK;
+    };
+    auto per_pair = [&](auto fn) -> int {
+        int rc = fork();
+        for (int i = 0; !rc && i < b->n; ++i) {
+            rc = fn(b->eng[i]);
+            if (rc) b->err = b->eng[i]->err;
+        }
+        const int rj = join();
+        return rc ? rc : rj;
+    };
+    int rc = per_pair([](piv_engine *e) { return do_prep(e); });
+    const piv_params &p0 = b->eng[0]->p;
+    for (int k = 0; !rc && k < 2; ++k) {
+        const int np = k ? p0.Npass2 : p0.Npass1;
+        if (np == 0) continue;
+        if (k == 1) rc = per_pair([](piv_engine *e) { return do_upsample(e); });
+        for (int j = 0; !rc && j < np; ++j) {
+            const bool deformed = !(k == 0 && j == 0);
+            rc = per_pair([&](piv_engine *e) -> int {
+                GridState &gs = e->grid[k];
+                if (!deformed) {
+                    CK(cudaMemsetAsync(gs.fx, 0, sizeof(float) * gs.gg.Nt_vec, e->stream));
+                    CK(cudaMemsetAsync(gs.fy, 0, sizeof(float) * gs.gg.Nt_vec, e->stream));
+                    return PIV_OK;
+                }
+                return do_deform(e, k);
+            });
+            for (auto &g : b->groups)
+                if (!rc && g.k == k && g.deformed == deformed) rc = batch_launch_group(b, g, g.variant);
+            if (rc) break;
+            rc = per_pair([&](piv_engine *e) {
+                const piv_params &p = e->p;
+                return k ? do_validate(e, 1, p.Npass2_median, p.minNneigh_p2, p.insert_threshold_p2, p.Npass2_smooth, 1)
+                         : do_validate(e, 0, p.Npass1_median, p.minNneigh_p1, p.insert_threshold_p1, p.Npass1_smooth, 1);
+            });
+        }
+    }
+    restore();
+    return rc;
+}
+
+// each group's tile variant, timed on the batch's own data after one eager run
+int batch_tune(piv_batch *b)
+{
+    int rc = batch_enqueue(b);
+    if (rc) return rc;
+    BCK(cudaStreamSynchronize(b->stream));
+    const char *env = getenv("PIV_AUTOTUNE");
+    if (env && env[0] == '0') return PIV_OK;
+    cudaEvent_t t0, t1;
+    BCK(cudaEventCreate(&t0));
+    BCK(cudaEventCreate(&t1));
+    for (auto &g : b->groups) {
+        float best = 0.f;
+        for (int v = 0; v < g.n_variants; ++v) {
+            if ((rc = batch_launch_group(b, g, v))) break;  // warm-up
+            BCK(cudaEventRecord(t0, b->stream));
+            for (int r = 0; r < 3 && !rc; ++r) rc = batch_launch_group(b, g, v);
+            BCK(cudaEventRecord(t1, b->stream));
+            BCK(cudaEventSynchronize(t1));
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, t0, t1);
+            g.tuned_ms[v] = ms / 3.f;
+            if (v == 0 || g.tuned_ms[v] < best) {
+                best = g.tuned_ms[v];
+                g.variant = v;
+            }
+        }
+        if (rc) break;
+    }
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    return rc;
+}
+
+}  // namespace
+
+extern "C" {
+
+int piv_batch_create(const piv_params *params, int n, piv_batch **out)
+{
+    if (!params || n < 1 || !out) return PIV_ERR_ARG;
+    *out = nullptr;
+    for (int i = 1; i < n; ++i)
+        if (params[i].Npass1 != params[0].Npass1 || params[i].Npass2 != params[0].Npass2) return PIV_ERR_ARG;
+    piv_batch *b = new piv_batch;
+    b->n = n;
+    b->eng.assign(n, nullptr);
+    cudaGetDevice(&b->device);
+    int rc = PIV_OK;
+    for (int i = 0; i < n && !rc; ++i) {
+        piv_params p = params[i];
+        p.device_id = b->device;
+        rc = piv_create(&p, &b->eng[i]);
+        if (rc) batch_err(b, rc, "pair %d: engine creation failed", i);
+    }
+    if (!rc) {
+        const int W = std::min(n, 8);
+        b->workers.resize(W);
+        b->ev_join.resize(W);
+        if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming) != cudaSuccess)
+            rc = PIV_ERR_CUDA;
+        for (int w = 0; w < W && !rc; ++w)
+            if (cudaStreamCreateWithFlags(&b->workers[w], cudaStreamNonBlocking) != cudaSuccess ||
+                cudaEventCreateWithFlags(&b->ev_join[w], cudaEventDisableTiming) != cudaSuccess)
+                rc = PIV_ERR_CUDA;
+    }
+    if (!rc) {
+        // every pass buffer up front (deformed frames of both grids)
+        for (int i = 0; i < n && !rc; ++i)
+            for (int k = 0; k < 2 && !rc; ++k) {
+                GridState &gs = b->eng[i]->grid[k];
+                const int np = k ? b->eng[i]->p.Npass2 : b->eng[i]->p.Npass1;
+                if (!gs.def && (k == 1 ? np > 0 : np > 1))
+                    rc = dalloc(b->eng[i], &gs.def, (size_t)gs.def_pitch * gs.gg.Ny_aug);
+            }
+    }
+    if (!rc) rc = batch_build_groups(b);
+    if (rc) {
+        batch_free(b);
+        delete b;
+        return rc;
+    }
+    *out = b;
+    return PIV_OK;
+}
+
+int piv_batch_destroy(piv_batch *b)
+{
+    if (!b) return PIV_ERR_ARG;
+    cudaSetDevice(b->device);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    batch_free(b);
+    delete b;
+    return PIV_OK;
+}
+
+const char *piv_batch_last_error(const piv_batch *b) { return b ? b->err.c_str() : "null batch"; }
+
+int piv_batch_engine(piv_batch *b, int i, piv_engine **e)
+{
+    if (!b || !e || i < 0 || i >= b->n) return PIV_ERR_ARG;
+    *e = b->eng[i];
+    return PIV_OK;
+}
+
+int piv_batch_run(piv_batch *b)
+{
+    if (!b) return PIV_ERR_ARG;
+    cudaSetDevice(b->device);
+    for (piv_engine *e : b->eng)
+        if (e->pending_slot >= 0) return batch_err(b, PIV_ERR_STATE, "a queued pair is pending on an engine");
+    int rc;
+    if (!b->tuned) {
+        if ((rc = batch_tune(b))) return rc;
+        b->tuned = true;
+    }
+    std::vector<const uint8_t *> in;
+    for (piv_engine *e : b->eng) {
+        in.push_back(e->d_in1);
+        in.push_back(e->d_in2);
+    }
+    if (!b->exec || in != b->graph_in) {
+        if (b->exec) cudaGraphExecDestroy(b->exec);
+        b->exec = nullptr;
+        cudaGraph_t g = nullptr;
+        BCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+        rc = batch_enqueue(b);
+        cudaError_t ce = cudaStreamEndCapture(b->stream, &g);
+        if (rc) {
+            if (g) cudaGraphDestroy(g);
+            return rc;
+        }
+        if (ce != cudaSuccess) return batch_err(b, PIV_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(ce));
+        cudaError_t ie = cudaGraphInstantiate(&b->exec, g, 0);
+        cudaGraphDestroy(g);
+        if (ie != cudaSuccess) return batch_err(b, PIV_ERR_CUDA, "graph instantiation failed: %s", cudaGetErrorString(ie));
+        b->graph_in = in;
+    }
+    BCK(cudaGraphLaunch(b->exec, b->stream));
+    for (piv_engine *e : b->eng) {
+        e->prepared = true;
+        e->grid[0].has_pass = e->p.Npass1 > 0;
+        e->grid[0].last_deformed = e->p.Npass1 > 1;
+        e->grid[1].has_pass = e->p.Npass2 > 0;
+        e->grid[1].last_deformed = true;
+    }
+    return PIV_OK;
+}
+
+int piv_batch_synchronize(piv_batch *b)
+{
+    if (!b) return PIV_ERR_ARG;
+    cudaSetDevice(b->device);
+    BCK(cudaStreamSynchronize(b->stream));
+    for (int i = 0; i < b->n; ++i) {
+        int rc = piv_synchronize(b->eng[i]);
+        if (rc) return batch_err(b, rc, "pair %d: %s", i, b->eng[i]->err.c_str());
+    }
+    return PIV_OK;
+}
+
+int piv_batch_stream(const piv_batch *b, void **stream)
+{
+    if (!b || !stream) return PIV_ERR_ARG;
+    *stream = b->stream;
+    return PIV_OK;
+}
+
+int piv_batch_groups(const piv_batch *b, int max, int *wsx, int *wsy, int *grid, int *deformed, int *pairs,
+                     int *variant, int *windows_per_cta, int *n_groups)
+{
+    if (!b || !n_groups) return PIV_ERR_ARG;
+    *n_groups = (int)b->groups.size();
+    for (int i = 0; i < *n_groups && i < max; ++i) {
+        const auto &g = b->groups[i];
+        if (wsx) wsx[i] = g.wsx;
+        if (wsy) wsy[i] = g.wsy;
+        if (grid) grid[i] = g.k;
+        if (deformed) deformed[i] = g.deformed ? 1 : 0;
+        if (pairs) pairs[i] = (int)g.pairs.size();
+        if (variant) variant[i] = g.variant;
+        if (windows_per_cta) windows_per_cta[i] = xcorr_batch_windows_per_cta(g.wsx, g.wsy, g.variant);
+    }
     return PIV_OK;
 }
 

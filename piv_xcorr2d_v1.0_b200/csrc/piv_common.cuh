@@ -128,10 +128,25 @@ struct XcorrArgs {
     int *status;               // device status word (tensor-core path: kStatusMmaWait), may be null
 };
 
+// Batch of pairs sharing a window shape (persistent batch launch): pairs[n] in device
+// memory, first[n + 1] the prefix sums of each pair's CTA-sized window batches.
+struct XcorrBatch {
+    const XcorrArgs *pairs;
+    const int *first;
+    int n, items;
+};
+
 // Launches the fused correlation + peak kernel for the window range of a.
 // deformed: frame 2 comes from a.def (float) instead of a.f2 (uint8).  variant selects
 // one of the shape's instantiations (windows per CTA, threads per CTA); 0 = default.
 cudaError_t launch_xcorr(const XcorrArgs &a, bool deformed, cudaStream_t s, const char **why, int variant);
+// Persistent batch launch over pairs sharing the window shape (wsx, wsy): variants
+// 0 .. xcorr_batch_variants() - 1, each with its windows per CTA (items are batches of
+// that many windows).  K: top-K width (4 or 8).
+int xcorr_batch_variants(int wsx, int wsy);
+int xcorr_batch_windows_per_cta(int wsx, int wsy, int variant);
+cudaError_t launch_xcorr_batch(int wsx, int wsy, int variant, const XcorrBatch &b, bool deformed, int K,
+                               cudaStream_t s, const char **why);
 bool xcorr_supported(int ws_x, int ws_y);
 int xcorr_variants(int ws_x, int ws_y);
 bool xcorr_variant_shape(int ws_x, int ws_y, int variant, int *windows_per_cta, int *threads_per_cta);

@@ -62,6 +62,41 @@ cudaError_t launch_shape(const XcorrArgs &a, bool deformed, int K, cudaStream_t 
 PIV_XCORR_VARIANTS(PIV_X)
 #undef PIV_X
 
+// Variants of the persistent batch launch (two per shape; the batch autotuner picks one
+// per shape group).
+template <int WSX, int WSY, int B, int NT>
+cudaError_t launch_shape_batch(const XcorrBatch &b, bool deformed, int K, cudaStream_t s);
+#define PIV_XCORR_BATCH_VARIANTS(X) \
+    X(8, 8, 32, 128) \
+    X(8, 8, 16, 128) \
+    X(12, 12, 16, 96) \
+    X(12, 12, 8, 96) \
+    X(16, 16, 16, 128) \
+    X(16, 16, 8, 128) \
+    X(24, 24, 8, 96) \
+    X(24, 24, 4, 96) \
+    X(32, 32, 4, 128) \
+    X(32, 32, 8, 128) \
+    X(48, 48, 4, 96) \
+    X(48, 48, 2, 96) \
+    X(64, 64, 2, 128) \
+    X(64, 64, 4, 128) \
+    X(48, 24, 4, 96) \
+    X(48, 24, 2, 64) \
+    X(24, 48, 4, 96) \
+    X(24, 48, 2, 64) \
+    X(32, 16, 8, 128) \
+    X(32, 16, 4, 64) \
+    X(16, 32, 8, 128) \
+    X(16, 32, 4, 64) \
+    X(64, 32, 4, 128) \
+    X(64, 32, 2, 64) \
+    X(32, 64, 4, 128) \
+    X(32, 64, 2, 64)
+#define PIV_X(WX, WY, B, NT) extern template cudaError_t launch_shape_batch<WX, WY, B, NT>(const XcorrBatch &, bool, int, cudaStream_t);
+PIV_XCORR_BATCH_VARIANTS(PIV_X)
+#undef PIV_X
+
 namespace {
 struct Variant {
     int wsx, wsy, B, NT;
@@ -102,6 +137,53 @@ bool xcorr_variant_shape(int wsx, int wsy, int variant, int *B, int *NT)
     if (B) *B = v->B;
     if (NT) *NT = v->NT;
     return true;
+}
+
+namespace {
+struct BatchVariant {
+    int wsx, wsy, B, NT;
+    cudaError_t (*fn)(const XcorrBatch &, bool, int, cudaStream_t);
+};
+const BatchVariant kBatchVariants[] = {
+#define PIV_X(WX, WY, B, NT) {WX, WY, B, NT, &launch_shape_batch<WX, WY, B, NT>},
+    PIV_XCORR_BATCH_VARIANTS(PIV_X)
+#undef PIV_X
+};
+
+const BatchVariant *find_batch(int wsx, int wsy, int v)
+{
+    int seen = 0;
+    for (const BatchVariant &b : kBatchVariants)
+        if (b.wsx == wsx && b.wsy == wsy) {
+            if (seen == v) return &b;
+            ++seen;
+        }
+    return nullptr;
+}
+}  // namespace
+
+int xcorr_batch_variants(int wsx, int wsy)
+{
+    int n = 0;
+    for (const BatchVariant &b : kBatchVariants) n += (b.wsx == wsx && b.wsy == wsy);
+    return n;
+}
+
+int xcorr_batch_windows_per_cta(int wsx, int wsy, int variant)
+{
+    const BatchVariant *v = find_batch(wsx, wsy, variant);
+    return v ? v->B : 0;
+}
+
+cudaError_t launch_xcorr_batch(int wsx, int wsy, int variant, const XcorrBatch &b, bool deformed, int K,
+                               cudaStream_t s, const char **why)
+{
+    const BatchVariant *v = find_batch(wsx, wsy, variant);
+    if (!v) {
+        if (why) *why = "window shape has no batch launch";
+        return cudaErrorInvalidValue;
+    }
+    return v->fn(b, deformed, K, s);
 }
 
 cudaError_t launch_xcorr(const XcorrArgs &a, bool deformed, cudaStream_t s, const char **why, int variant)

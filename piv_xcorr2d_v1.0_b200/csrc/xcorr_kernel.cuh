@@ -31,6 +31,7 @@
 //       count, register top-K (value desc, then lower index), 3-point Gaussian fit
 //       with an FP64 log-ratio denominator, predictor, limits, NaN/Inf removal.
 #pragma once
+#include <algorithm>
 #include <cfloat>
 #include <climits>
 
@@ -379,8 +380,10 @@ constexpr int xcorr_min_ctas()
     return (WSX == 32 && WSY == 32 && B == 4 && NT == 128) ? 6 : 1;
 }
 
+// The whole correlation of the CTA-sized window batch `blk` of one launch (P1..P5); the
+// single-pair kernel runs it for its block, the batch kernel for every item it takes.
 template <int WSX, int WSY, int B, int NT, int K, bool DEF>
-__global__ void __launch_bounds__(NT, (xcorr_min_ctas<WSX, WSY, B, NT>())) xcorr_peak_kernel(const XcorrArgs a)
+__device__ __forceinline__ void xcorr_body(const XcorrArgs &a, const int blk)
 {
     static_assert(B % 2 == 0, "windows are processed in pairs");
     static_assert(NT % 32 == 0, "the peak stage works in whole warps");
@@ -392,7 +395,7 @@ __global__ void __launch_bounds__(NT, (xcorr_min_ctas<WSX, WSY, B, NT>())) xcorr
 
     const GridGeom &g = a.g;
     const int tid = threadIdx.x;
-    const int w_base = a.w_first + blockIdx.x * B;
+    const int w_base = a.w_first + blk * B;
 
     // ---------------- P1: row gather + forward row FFT ----------------
     for (int t = tid; t < B * WSY; t += NT) {
@@ -552,6 +555,39 @@ __global__ void __launch_bounds__(NT, (xcorr_min_ctas<WSX, WSY, B, NT>())) xcorr
     }
 }
 
+template <int WSX, int WSY, int B, int NT, int K, bool DEF>
+__global__ void __launch_bounds__(NT, (xcorr_min_ctas<WSX, WSY, B, NT>())) xcorr_peak_kernel(const XcorrArgs a)
+{
+    xcorr_body<WSX, WSY, B, NT, K, DEF>(a, blockIdx.x);
+}
+
+// Persistent batch form: the CTA-sized window batches ("items") of many pairs with the
+// same window shape in one launch.  Pair i owns items [first[i], first[i+1]); a CTA takes
+// items blockIdx.x, blockIdx.x + gridDim.x, ... and reads its pair's arguments from
+// global memory.
+// (one resident CTA fewer than the single-pair kernel where that one asks for more than
+// one: the item loop keeps a few more values live, which spilled at the tighter bound)
+template <int WSX, int WSY, int B, int NT>
+constexpr int xcorr_batch_min_ctas()
+{
+    return xcorr_min_ctas<WSX, WSY, B, NT>() > 1 ? xcorr_min_ctas<WSX, WSY, B, NT>() - 1 : 1;
+}
+
+template <int WSX, int WSY, int B, int NT, int K, bool DEF>
+__global__ void __launch_bounds__(NT, (xcorr_batch_min_ctas<WSX, WSY, B, NT>())) xcorr_batch_kernel(const XcorrBatch b)
+{
+    for (int it = blockIdx.x; it < b.items; it += gridDim.x) {
+        int lo = 0, hi = b.n - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (b.first[mid] <= it) lo = mid;
+            else hi = mid - 1;
+        }
+        xcorr_body<WSX, WSY, B, NT, K, DEF>(b.pairs[lo], it - b.first[lo]);
+        __syncthreads();  // the next item reuses the shared buffers
+    }
+}
+
 // ------------------------------------------------------------------------------
 // Launch of one instantiated shape (explicitly instantiated in xcorr_shape_*.cu).
 // ------------------------------------------------------------------------------
@@ -575,6 +611,35 @@ cudaError_t launch_shape(const XcorrArgs &a, bool deformed, int K, cudaStream_t 
     } else {
         if (deformed) go(xcorr_peak_kernel<WSX, WSY, B, NT, 8, true>);
         else go(xcorr_peak_kernel<WSX, WSY, B, NT, 8, false>);
+    }
+    return e;
+}
+
+// Launch of a batch: items = sum over pairs of ceil(windows / B), first[] their prefix
+// sums on the device; a persistent grid of (resident CTAs per SM) x SMs, at most items.
+template <int WSX, int WSY, int B, int NT>
+cudaError_t launch_shape_batch(const XcorrBatch &b, bool deformed, int K, cudaStream_t s)
+{
+    if (b.items <= 0) return cudaSuccess;
+    const size_t smem = (size_t)B * WSY * (WSX + 1) * sizeof(float2);
+    cudaError_t e = cudaSuccess;
+    auto go = [&](auto kern) {
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return;
+        int per_sm = 0, dev = 0, sms = 0;
+        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, smem)) != cudaSuccess) return;
+        if ((e = cudaGetDevice(&dev)) != cudaSuccess) return;
+        if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return;
+        const int grid = std::max(1, std::min(b.items, std::max(per_sm, 1) * sms));
+        kern<<<grid, NT, smem, s>>>(b);
+        e = cudaGetLastError();
+    };
+    if (K <= 4) {
+        if (deformed) go(xcorr_batch_kernel<WSX, WSY, B, NT, 4, true>);
+        else go(xcorr_batch_kernel<WSX, WSY, B, NT, 4, false>);
+    } else {
+        if (deformed) go(xcorr_batch_kernel<WSX, WSY, B, NT, 8, true>);
+        else go(xcorr_batch_kernel<WSX, WSY, B, NT, 8, false>);
     }
     return e;
 }

@@ -1,5 +1,5 @@
 // Fused correlation kernel, 16x16 windows: the (windows per CTA, threads per CTA)
-// variants the autotuner chooses from.
+// variants the autotuner chooses from, and the batch-launch variants.
 #include "xcorr_kernel.cuh"
 
 namespace piv {
@@ -7,4 +7,6 @@ template cudaError_t launch_shape<16, 16, 16, 128>(const XcorrArgs &, bool, int,
 template cudaError_t launch_shape<16, 16, 8, 128>(const XcorrArgs &, bool, int, cudaStream_t);
 template cudaError_t launch_shape<16, 16, 16, 256>(const XcorrArgs &, bool, int, cudaStream_t);
 template cudaError_t launch_shape<16, 16, 4, 64>(const XcorrArgs &, bool, int, cudaStream_t);
+template cudaError_t launch_shape_batch<16, 16, 16, 128>(const XcorrBatch &, bool, int, cudaStream_t);
+template cudaError_t launch_shape_batch<16, 16, 8, 128>(const XcorrBatch &, bool, int, cudaStream_t);
 }

@@ -1,5 +1,5 @@
 // Fused correlation kernel, 64x64 windows: the (windows per CTA, threads per CTA)
-// variants the autotuner chooses from.
+// variants the autotuner chooses from, and the batch-launch variants.
 #include "xcorr_kernel.cuh"
 
 namespace piv {
@@ -7,4 +7,6 @@ template cudaError_t launch_shape<64, 64, 2, 128>(const XcorrArgs &, bool, int, 
 template cudaError_t launch_shape<64, 64, 4, 128>(const XcorrArgs &, bool, int, cudaStream_t);
 template cudaError_t launch_shape<64, 64, 2, 64>(const XcorrArgs &, bool, int, cudaStream_t);
 template cudaError_t launch_shape<64, 64, 4, 256>(const XcorrArgs &, bool, int, cudaStream_t);
+template cudaError_t launch_shape_batch<64, 64, 2, 128>(const XcorrBatch &, bool, int, cudaStream_t);
+template cudaError_t launch_shape_batch<64, 64, 4, 128>(const XcorrBatch &, bool, int, cudaStream_t);
 }
