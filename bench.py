@@ -18,6 +18,9 @@ pair: 113,300 (412 x 275).
   learned, learned_split_bf16  the learned form of the same pair (piv_run_pair_learned:
          trained predictor instead of the grid-1 passes, grid-2 passes on FP32 SIMT or
          split-BF16 tensor cores, judge with fallback), per-pair CUDA events.
+  batch  64 pairs of uneven size and window shape through piv_batch_run (one persistent
+         correlation launch per pass and window shape, one graph), against the same
+         engines one pair at a time.
   --impl reference  the reference's own engine (xcorr2d_multi + mhe_gpu, compiled for
          sm_100a from its sources) on the same pair through its public methods.
 
@@ -209,6 +212,109 @@ def learned_form(P, e, ext, flush, args, s, path, plain_ms):
             else str(args.weights)}
 
 
+BATCH_SIZES = [(1024, 1024)] * 16 + [(2048, 1536)] * 16 + [(4096, 2160)] * 16 + [(6600, 4400)] * 16
+
+
+def batch_workload(P, seed=3):
+    """64 pairs of uneven size: 16 each at 1024x1024, 2048x1536, 4096x2160 and 6600x4400;
+    0.02-0.08 particles/px; sums of 8 Fourier modes (wavelengths 200-2000 px, at most
+    12 px); grid-2 windows drawn from {16, 24, 32, 64} at 50 or 75 % overlap, grid 1 at
+    min(2 ws, 64) with the same overlap, 2 + 3 passes, MHE on."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k, (Nx, Ny) in enumerate(BATCH_SIZES):
+        ws2 = int(rng.choice([16, 24, 32, 64]))
+        ov = float(rng.choice([0.5, 0.75]))
+        ws1 = min(2 * ws2, 64)
+        sp = lambda ws: int(round(ws * (1 - ov)))
+        p = P.default_params(Nx=Nx, Ny=Ny, if_mhe=1, mhe_ws=40, mhe_thresh=0.91, ws_x1=ws1, ws_y1=ws1,
+                             spacing_x1=sp(ws1), spacing_y1=sp(ws1), Npass1=2, ws_x2=ws2, ws_y2=ws2,
+                             spacing_x2=sp(ws2), spacing_y2=sp(ws2), Npass2=3, Nsec_cc=1,
+                             insert_threshold_p1=2.0, insert_threshold_p2=2.0)
+        s = P.synth_params(Nx, Ny, ppp=float(rng.uniform(0.02, 0.08)), field=P.PIV_FIELD_FOURIER, a=200.0,
+                           b=2000.0, c=12.0, seed=5000 + k)
+        out.append((p, s))
+    return out
+
+
+def batch_form(P, args, flush):
+    """The uneven batch: one graph with one persistent correlation launch per pass and window
+    shape (piv_batch_run), against the same engines run one pair at a time (each pair's own
+    graph, piv_run_pair).  Device time by CUDA events; frames in HBM; L2 flushed first."""
+    import torch
+
+    pairs = batch_workload(P)
+    b = P.Batch([p for p, _ in pairs])
+    frames = []
+    for e, (p, s) in zip(b.engines, pairs):
+        n = s.Nx * s.Ny
+        d1 = torch.empty(n, dtype=torch.uint8, device="cuda")
+        d2 = torch.empty_like(d1)
+        scratch = torch.empty(2 * n, dtype=torch.float32, device="cuda")
+        P.synth_pair_device(s, d1, d2, scratch)
+        frames.append((d1, d2))
+        del scratch
+    torch.cuda.synchronize()
+    for e, (d1, d2) in zip(b.engines, frames):
+        e.set_device_images(d1.data_ptr(), d2.data_ptr())
+    nvec = sum(e.geom["Nt_vec"][1] for e in b.engines)
+    ext = torch.cuda.ExternalStream(b.stream())
+    for _ in range(args.warmup):
+        b.run()
+        b.synchronize()
+    reps = max(3, min(args.steps, 10))
+    ms_b = []
+    for _ in range(reps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0.record(ext)
+        b.run()
+        t1.record(ext)
+        t1.synchronize()
+        ms_b.append(t0.elapsed_time(t1))
+    b.synchronize()
+    se, cnt = 0.0, 0
+    for e, (p, s) in zip(b.engines, pairs):
+        x, y, dx, dy, v = e.field(3)
+        u, w = P.synth_field(s, x, y)
+        ok = v == 1
+        se += float((((dx - u) ** 2 + (dy - w) ** 2)[ok]).sum())
+        cnt += int(ok.sum())
+    # the same pairs one at a time, each its own captured graph
+    for e in b.engines:
+        e.run_pair()
+        e.synchronize()
+    ms_p = []
+    for _ in range(reps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        tot = 0.0
+        for e in b.engines:
+            es = torch.cuda.ExternalStream(e.stream())
+            t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            t0.record(es)
+            e.run_pair()
+            t1.record(es)
+            t1.synchronize()
+            tot += t0.elapsed_time(t1)
+        ms_p.append(tot)
+    groups = b.groups()
+    b.close()
+    mb, mp = statistics.median(ms_b), statistics.median(ms_p)
+    return {"value": round(nvec / (mb * 1e-3), 1), "unit": UNIT, "ms_per_batch": round(mb, 3),
+            "pairs": len(pairs), "vectors_per_batch": nvec,
+            "one_pair_at_a_time": {"value": round(nvec / (mp * 1e-3), 1), "ms_per_batch": round(mp, 3)},
+            "speedup": round(mp / mb, 3), "correlation_launches_per_pass": {
+                "grid1_first": sum(1 for g in groups if g["grid"] == 0 and not g["deformed"]),
+                "grid1_deformed": sum(1 for g in groups if g["grid"] == 0 and g["deformed"]),
+                "grid2": sum(1 for g in groups if g["grid"] == 1)},
+            "groups": groups, "accuracy_rms_px": round(float(np.sqrt(se / max(cnt, 1))), 4),
+            "workload": "64 uneven pairs: 16 each at 1024x1024, 2048x1536, 4096x2160, 6600x4400; "
+                        "ws2 in {16,24,32,64} at 50/75 % overlap, ws1 = min(2 ws2, 64); 2+3 passes; MHE on; "
+                        "Fourier fields up to 12 px", "reps": reps}
+
+
 def replicas():
     load_pkg()
     import piv_b200.replicas as R
@@ -319,6 +425,8 @@ def run_ours(args, rank, world, local):
         out["learned_split_bf16"] = learned_form(P, e, ext, flush, args, s_true, P.PIV_XCORR_TC_SPLIT, plain_ms)
     else:
         out["learned"] = {"unavailable": f"no predictor weights at {args.weights}"}
+    if not args.no_batch:
+        out["batch"] = batch_form(P, args, flush)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(P, f1, f2, args.cpu_rows)
     e.close()
@@ -372,6 +480,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-rows", type=int, default=1024, help="rows of the pair the CPU baseline processes")
+    ap.add_argument("--no-batch", action="store_true", help="skip the 64-pair uneven batch line")
     ap.add_argument("--weights", default=str(PKG_DIR / "weights" / "predictor.bin"),
                     help="learned-predictor weights (piv_xcorr2d_v1.0_b200/train_predictor.py)")
     args = ap.parse_args()

@@ -128,7 +128,7 @@ struct XcorrArgs {
     int *status;               // device status word (tensor-core path: kStatusMmaWait), may be null
 };
 
-// Batch of pairs sharing a window shape (persistent batch launch): pairs[n] in device
+// Batch of pairs sharing a window shape (one launch for all of them): pairs[n] in device
 // memory, first[n + 1] the prefix sums of each pair's CTA-sized window batches.
 struct XcorrBatch {
     const XcorrArgs *pairs;
