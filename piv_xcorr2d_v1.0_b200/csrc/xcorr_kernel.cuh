@@ -31,7 +31,6 @@
 //       count, register top-K (value desc, then lower index), 3-point Gaussian fit
 //       with an FP64 log-ratio denominator, predictor, limits, NaN/Inf removal.
 #pragma once
-#include <algorithm>
 #include <cfloat>
 #include <climits>
 
@@ -380,188 +379,12 @@ constexpr int xcorr_min_ctas()
     return (WSX == 32 && WSY == 32 && B == 4 && NT == 128) ? 6 : 1;
 }
 
-// The whole correlation of the CTA-sized window batch `blk` of one launch (P1..P5); the
-// single-pair kernel runs it for its block, the batch kernel for every item it takes.
-template <int WSX, int WSY, int B, int NT, int K, bool DEF>
-__device__ __forceinline__ void xcorr_body(const XcorrArgs &a, const int blk)
-{
-    static_assert(B % 2 == 0, "windows are processed in pairs");
-    static_assert(NT % 32 == 0, "the peak stage works in whole warps");
-    constexpr int LDX = WSX + 1;   // complex row stride (odd -> conflict-free rows and columns)
-    constexpr int WIN = WSY * LDX; // complex elements per window buffer
-    constexpr int LDF = WSX + 1;   // float row stride of the correlation planes
-    constexpr float inv_n = 1.0f / (float)(WSX * WSY);
-    extern __shared__ float2 sm[];
-
-    const GridGeom &g = a.g;
-    // read through an opaque move: in the batch kernel's item loop, values derived from the
-    // thread index would otherwise be hoisted out of the loop and held through every phase
-    int tid;
-    asm volatile("mov.u32 %0, %%tid.x;" : "=r"(tid));
-    const int w_base = a.w_first + blk * B;
-
-    // ---------------- P1: row gather + forward row FFT ----------------
-    for (int t = tid; t < B * WSY; t += NT) {
-        const int b = t / WSY, r = t - b * WSY;
-        const int w = w_base + b;
-        float2 z[WSX];
-        if (w < a.w_end) {
-            const int iy = w / g.Nx_vec, ix = w - iy * g.Nx_vec;
-            const int x0 = ix * g.sp_x - g.Nx_left + a.f1.mx;
-            const int y1 = iy * g.sp_y + r - g.Ny_left + a.f1.my;
-            float v1[WSX], v2[WSX];
-            load_u8_row<WSX>(a.f1.base + (size_t)y1 * a.f1.pitch + x0, v1);
-            if constexpr (DEF) {
-                load_f32_row<WSX>(a.def + (size_t)(iy * g.sp_y + r) * a.def_pitch + ix * g.sp_x, v2);
-            } else {
-                load_u8_row<WSX>(a.f2.base + (size_t)y1 * a.f2.pitch + x0, v2);
-            }
-#pragma unroll
-            for (int i = 0; i < WSX; ++i) z[i] = make_float2(v1[i], v2[i]);
-        } else {
-#pragma unroll
-            for (int i = 0; i < WSX; ++i) z[i] = make_float2(0.f, 0.f);
-        }
-        fft<WSX, false>(z);
-        float2 *row = sm + (b * WSY + r) * LDX;
-#pragma unroll
-        for (int i = 0; i < WSX; ++i) row[i] = z[i];
-    }
-    __syncthreads();
-
-    // ---------------- P2: forward column FFT ----------------
-    for (int t = tid; t < B * WSX; t += NT) {
-        const int b = t / WSX, c = t - b * WSX;
-        float2 *col = sm + b * WIN + c;
-        float2 z[WSY];
-#pragma unroll
-        for (int r = 0; r < WSY; ++r) z[r] = col[r * LDX];
-        fft<WSY, false>(z);
-#pragma unroll
-        for (int r = 0; r < WSY; ++r) col[r * LDX] = z[r];
-    }
-    __syncthreads();
-
-    // ---------------- P3: cross spectrum of a window pair + inverse column FFT ----------------
-    // A pair task has one column per window pair, so half of the CTA would idle: for
-    // columns of 32 and more (measured gains at 32 and 64) and where the CTA has the
-    // threads, a lane pair shares each column (rows split by parity, fft2t).
-    constexpr bool P3_PAIRED = 2 * (B / 2) * WSX <= NT && WSY % 4 == 0 && WSY >= 32;
-    static_assert((B / 2) * WSX <= NT, "one P3 task per thread");
-    {
-        constexpr int NR = P3_PAIRED ? WSY / 2 : WSY;  // rows per thread
-        // pair: lanes l and l + 16 of a warp (16 tasks per warp)
-        const int task = P3_PAIRED ? (tid >> 5) * 16 + (tid & 15) : tid, half = P3_PAIRED ? (tid >> 4) & 1 : 0;
-        const bool active = task < (B / 2) * WSX;
-        const unsigned mask = __ballot_sync(0xffffffffu, active);
-        const int q = active ? task / WSX : 0, c = active ? task - (task / WSX) * WSX : 0;
-        const int cm = (WSX - c) % WSX;
-        float2 wv[NR];
-        if (active) {
-            const float2 *za = sm + (2 * q) * WIN, *zb = sm + (2 * q + 1) * WIN;
-#pragma unroll
-            for (int jj = 0; jj < NR; ++jj) {
-                const int r = P3_PAIRED ? 2 * jj + half : jj;
-                const int rm = (WSY - r) % WSY;
-                float2 A = za[r * LDX + c], M = za[rm * LDX + cm];
-                // C = Im(A*M)/2 + i*(|M|^2 - |A|^2)/4
-                float2 Ca = make_float2(0.5f * (A.x * M.y + A.y * M.x),
-                                        0.25f * ((M.x * M.x + M.y * M.y) - (A.x * A.x + A.y * A.y)));
-                A = zb[r * LDX + c];
-                M = zb[rm * LDX + cm];
-                float2 Cb = make_float2(0.5f * (A.x * M.y + A.y * M.x),
-                                        0.25f * ((M.x * M.x + M.y * M.y) - (A.x * A.x + A.y * A.y)));
-                wv[jj] = make_float2(Ca.x - Cb.y, Ca.y + Cb.x);  // C_a + i*C_b
-            }
-            if constexpr (P3_PAIRED) fft2t<WSY, true>(wv, half, mask);
-            else fft<WSY, true>(wv);
-        }
-        __syncthreads();  // every partner-column read is done
-        if (active) {
-            float2 *col = sm + (2 * q) * WIN + c;
-#pragma unroll
-            for (int m = 0; m < NR; ++m) {
-                const int r = P3_PAIRED ? fft2t_index<WSY>(m, half) : m;
-                col[r * LDX] = wv[m];
-            }
-        }
-    }
-    __syncthreads();
-
-    // ---------------- P4: inverse row FFT -> two shifted FP32 planes ----------------
-    // lane pairs per row for rows of 32 and more where the CTA has the threads (columns
-    // split by parity, fft2t)
-    constexpr bool P4_PAIRED = 2 * (B / 2) * WSY <= NT && WSX % 4 == 0 && WSX >= 32;
-    if constexpr (P4_PAIRED) {
-        const int task = (tid >> 5) * 16 + (tid & 15), half = (tid >> 4) & 1;  // lanes l, l + 16
-        const bool active = task < (B / 2) * WSY;
-        const unsigned mask = __ballot_sync(0xffffffffu, active);
-        if (active) {
-            const int q = task / WSY, r = task - q * WSY;
-            const float2 *row = sm + (2 * q) * WIN + r * LDX;
-            float2 z[WSX / 2];
-#pragma unroll
-            for (int jj = 0; jj < WSX / 2; ++jj) z[jj] = row[2 * jj + half];
-            fft2t<WSX, true>(z, half, mask);
-            float *pa = reinterpret_cast<float *>(sm + (2 * q + 1) * WIN);
-            float *pb = pa + WSY * LDF;
-            const int rs = (r + WSY / 2) % WSY;
-#pragma unroll
-            for (int m = 0; m < WSX / 2; ++m) {
-                const int is = (fft2t_index<WSX>(m, half) + WSX / 2) % WSX;
-                pa[rs * LDF + is] = fabsf(z[m].x) * inv_n;
-                pb[rs * LDF + is] = fabsf(z[m].y) * inv_n;
-            }
-        }
-    } else {
-        for (int t = tid; t < (B / 2) * WSY; t += NT) {
-            const int q = t / WSY, r = t - q * WSY;
-            const float2 *row = sm + (2 * q) * WIN + r * LDX;
-            float2 z[WSX];
-#pragma unroll
-            for (int i = 0; i < WSX; ++i) z[i] = row[i];
-            fft<WSX, true>(z);
-            float *pa = reinterpret_cast<float *>(sm + (2 * q + 1) * WIN);
-            float *pb = pa + WSY * LDF;
-            const int rs = (r + WSY / 2) % WSY;
-#pragma unroll
-            for (int i = 0; i < WSX; ++i) {
-                const int is = (i + WSX / 2) % WSX;
-                pa[rs * LDF + is] = fabsf(z[i].x) * inv_n;
-                pb[rs * LDF + is] = fabsf(z[i].y) * inv_n;
-            }
-        }
-    }
-    __syncthreads();
-
-    // ---------------- P5: peaks, warp per window (two for tall windows) ----------------
-    const int warp = tid >> 5, lane = tid & 31;
-    constexpr int NW = NT / 32;
-    if constexpr (WSY > 32 && NW >= 2 * B) {
-        // the even window buffers are free after P4: the halves' results go there
-        static_assert(B * sizeof(PeakPart[2]) <= WIN * sizeof(float2), "peak scratch fits in window buffer 0");
-        PeakPart(*parts)[2] = reinterpret_cast<PeakPart(*)[2]>(sm);
-        const int b = warp >> 1, part = warp & 1;
-        const int w = w_base + b;
-        const bool live = b < B && w < a.w_end;
-        const float *P = reinterpret_cast<const float *>(sm + ((b & ~1) + 1) * WIN) + (b & 1) * (WSY * LDF);
-        if (live) peak_window_part<WSX, WSY, K>(a, P, part, lane, parts[b][part]);
-        __syncthreads();
-        if (live && part == 0) peak_window_merge<WSX, WSY>(a, P, w, lane, parts[b]);
-    } else {
-        for (int b = warp; b < B; b += NW) {
-            const int w = w_base + b;
-            if (w >= a.w_end) continue;
-            const float *P = reinterpret_cast<const float *>(sm + ((b & ~1) + 1) * WIN) + (b & 1) * (WSY * LDF);
-            peak_window<WSX, WSY, K>(a, P, w, lane);
-        }
-    }
-}
 
 template <int WSX, int WSY, int B, int NT, int K, bool DEF>
 __global__ void __launch_bounds__(NT, (xcorr_min_ctas<WSX, WSY, B, NT>())) xcorr_peak_kernel(const XcorrArgs a)
 {
-    xcorr_body<WSX, WSY, B, NT, K, DEF>(a, blockIdx.x);
+    const unsigned blk = blockIdx.x;
+#include "xcorr_body.inc"
 }
 
 // Batch form: the CTA-sized window batches ("items") of many pairs with the same window
@@ -581,7 +404,9 @@ __global__ void __launch_bounds__(NT, (xcorr_min_ctas<WSX, WSY, B, NT>())) xcorr
         if (b.first[mid] <= it) lo = mid;
         else hi = mid - 1;
     }
-    xcorr_body<WSX, WSY, B, NT, K, DEF>(b.pairs[lo], it - b.first[lo]);
+    const XcorrArgs &a = b.pairs[lo];
+    const unsigned blk = it - b.first[lo];
+#include "xcorr_body.inc"
 }
 
 // ------------------------------------------------------------------------------
