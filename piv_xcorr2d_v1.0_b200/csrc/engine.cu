@@ -1549,9 +1549,7 @@ struct piv_batch {
         bool deformed = false;
         int wsx = 0, wsy = 0, K = 4;
         std::vector<int> pairs;
-        XcorrArgs *d_args = nullptr;
-        int *d_first[2] = {};
-        int items[2] = {};
+        std::vector<XcorrBatch> chunks[2];  // per tile variant: launches of <= kBatchMaxPairs pairs
         int n_variants = 0, variant = 0;
         float tuned_ms[2] = {};
     };
@@ -1586,11 +1584,6 @@ int batch_err(piv_batch *b, int code, const char *fmt, ...)
 void batch_free(piv_batch *b)
 {
     if (b->exec) cudaGraphExecDestroy(b->exec);
-    for (auto &g : b->groups) {
-        cudaFree(g.d_args);
-        cudaFree(g.d_first[0]);
-        cudaFree(g.d_first[1]);
-    }
     for (cudaStream_t s : b->workers) cudaStreamDestroy(s);
     for (cudaEvent_t ev : b->ev_join) cudaEventDestroy(ev);
     if (b->ev_fork) cudaEventDestroy(b->ev_fork);
@@ -1632,17 +1625,21 @@ int batch_build_groups(piv_batch *b)
         }
     for (auto &g : b->groups) {
         if (g.n_variants < 1) return batch_err(b, PIV_ERR_UNSUPPORTED, "window shape %dx%d has no batch launch", g.wsx, g.wsy);
-        std::vector<XcorrArgs> args;
-        for (int i : g.pairs) args.push_back(xcorr_args(b->eng[i], g.k));
-        BCK(cudaMalloc(&g.d_args, args.size() * sizeof(XcorrArgs)));
-        BCK(cudaMemcpy(g.d_args, args.data(), args.size() * sizeof(XcorrArgs), cudaMemcpyHostToDevice));
         for (int v = 0; v < g.n_variants; ++v) {
             const int B = xcorr_batch_windows_per_cta(g.wsx, g.wsy, v);
-            std::vector<int> first(1, 0);
-            for (const XcorrArgs &a : args) first.push_back(first.back() + (a.w_end - a.w_first + B - 1) / B);
-            g.items[v] = first.back();
-            BCK(cudaMalloc(&g.d_first[v], first.size() * sizeof(int)));
-            BCK(cudaMemcpy(g.d_first[v], first.data(), first.size() * sizeof(int), cudaMemcpyHostToDevice));
+            for (size_t c0 = 0; c0 < g.pairs.size(); c0 += kBatchMaxPairs) {
+                g.chunks[v].emplace_back();
+                XcorrBatch &xb = g.chunks[v].back();
+                memset(&xb, 0, sizeof(xb));
+                xb.n = (int)std::min(g.pairs.size() - c0, (size_t)kBatchMaxPairs);
+                xb.first[0] = 0;
+                for (int j = 0; j < xb.n; ++j) {
+                    xb.pairs[j] = xcorr_args(b->eng[g.pairs[c0 + j]], g.k);
+                    const int nw = xb.pairs[j].w_end - xb.pairs[j].w_first;
+                    xb.first[j + 1] = xb.first[j] + (nw + B - 1) / B;
+                }
+                xb.items = xb.first[xb.n];
+            }
         }
     }
     return PIV_OK;
@@ -1650,14 +1647,12 @@ int batch_build_groups(piv_batch *b)
 
 int batch_launch_group(piv_batch *b, const piv_batch::Group &g, int variant)
 {
-    XcorrBatch xb;
-    xb.pairs = g.d_args;
-    xb.first = g.d_first[variant];
-    xb.n = (int)g.pairs.size();
-    xb.items = g.items[variant];
-    const char *why = nullptr;
-    cudaError_t c = launch_xcorr_batch(g.wsx, g.wsy, variant, xb, g.deformed, g.K, b->stream, &why);
-    if (c != cudaSuccess) return batch_err(b, PIV_ERR_CUDA, "batch correlation: %s", why ? why : cudaGetErrorString(c));
+    for (const XcorrBatch &xb : g.chunks[variant]) {
+        const char *why = nullptr;
+        cudaError_t c = launch_xcorr_batch(g.wsx, g.wsy, variant, xb, g.deformed, g.K, b->stream, &why);
+        if (c != cudaSuccess)
+            return batch_err(b, PIV_ERR_CUDA, "batch correlation: %s", why ? why : cudaGetErrorString(c));
+    }
     return PIV_OK;
 }
 

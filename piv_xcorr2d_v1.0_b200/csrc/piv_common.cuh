@@ -128,11 +128,14 @@ struct XcorrArgs {
     int *status;               // device status word (tensor-core path: kStatusMmaWait), may be null
 };
 
-// Batch of pairs sharing a window shape (one launch for all of them): pairs[n] in device
-// memory, first[n + 1] the prefix sums of each pair's CTA-sized window batches.
+// Batch of pairs sharing a window shape (one launch for all of them), passed whole as the
+// kernel's parameter (about 24 KB, under the 32 KB parameter limit) so that the pairs'
+// arguments are read from the constant bank: pairs[n], first[n + 1] the prefix sums of
+// each pair's CTA-sized window batches.  Larger groups take several launches.
+constexpr int kBatchMaxPairs = 96;
 struct XcorrBatch {
-    const XcorrArgs *pairs;
-    const int *first;
+    XcorrArgs pairs[kBatchMaxPairs];
+    int first[kBatchMaxPairs + 1];
     int n, items;
 };
 
