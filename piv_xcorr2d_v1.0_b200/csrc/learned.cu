@@ -228,7 +228,7 @@ struct ConvIn {
 struct ConvFwd {
     ConvIn in;
     int N, Ho, Wo, stride;
-    const __nv_bfloat16 *w;
+    const __nv_bfloat16 *w;  // [ci][tap][co] (the forward's layout; 16-byte aligned)
     const float *bias;
     int cout;
     float *out;
@@ -302,12 +302,31 @@ __global__ void __launch_bounds__(256) conv_fwd_kernel(const ConvFwd c)
     for (int ci = warp; ci < cin; ci += 2 * NW) {
         const int cj = ci + NW;
         const bool two = cj < cin;
-        for (int e = lane; e < 9 * COT; e += 32) {
-            const int co = e / 9, tap = e - co * 9;
-            const bool ok = co0 + co < c.cout;
-            const size_t base = (size_t)(co0 + co) * cin * 9 + tap;
-            wsm[warp][0][tap][co] = ok ? __bfloat162float(c.w[base + (size_t)ci * 9]) : 0.f;
-            wsm[warp][1][tap][co] = ok && two ? __bfloat162float(c.w[base + (size_t)cj * 9]) : 0.f;
+        // both channels' weights: for each tap a contiguous run of COT output channels
+        if constexpr (COT % 8 == 0) {
+            constexpr int Q = COT / 8;  // 16-byte chunks per run
+            for (int e = lane; e < 2 * 9 * Q; e += 32) {
+                const int ch = e / (9 * Q), r = e - ch * (9 * Q), tap = r / Q, q = r - tap * Q;
+                const int cc = ch ? cj : ci;
+                uint4 u = make_uint4(0u, 0u, 0u, 0u);
+                if (ch == 0 || two)
+                    u = __ldg(reinterpret_cast<const uint4 *>(c.w + ((size_t)cc * 9 + tap) * c.cout + co0) + q);
+                const __nv_bfloat162 *h = reinterpret_cast<const __nv_bfloat162 *>(&u);
+                float *dst = &wsm[warp][ch][tap][8 * q];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const float2 f = __bfloat1622float2(h[j]);
+                    dst[2 * j] = f.x;
+                    dst[2 * j + 1] = f.y;
+                }
+            }
+        } else {
+            for (int e = lane; e < 2 * 9 * COT; e += 32) {
+                const int ch = e / (9 * COT), r = e - ch * (9 * COT), tap = r / COT, co = r - tap * COT;
+                const int cc = ch ? cj : ci;
+                const bool ok = co0 + co < c.cout && (ch == 0 || two);
+                wsm[warp][ch][tap][co] = ok ? __bfloat162float(c.w[((size_t)cc * 9 + tap) * c.cout + co0 + co]) : 0.f;
+            }
         }
         __syncwarp();
         float x0[9], x1[9];
@@ -571,6 +590,15 @@ __global__ void to_bf16_kernel(const float *p, __nv_bfloat16 *pb, size_t n)
     if (i < n) pb[i] = __float2bfloat16_rn(p[i]);
 }
 
+// One layer's weights [co][ci][tap] (FP32 masters) -> the forward's BF16 [ci][tap][co]
+__global__ void transpose_weights_kernel(const float *w, int cout, int cin, __nv_bfloat16 *wt)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;  // index in the source layout
+    if (i >= cout * cin * 9) return;
+    const int co = i / (cin * 9), r = i - co * (cin * 9), ci = r / 9, tap = r - ci * 9;
+    wt[((size_t)ci * 9 + tap) * cout + co] = __float2bfloat16_rn(w[i]);
+}
+
 __global__ void field_from_net_kernel(const float *out, int Nt, float *fx, float *fy, uint8_t *fv)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -629,6 +657,11 @@ struct piv_net {
     size_t w_off[kLayers] = {}, b_off[kLayers] = {};
     float *params = nullptr, *grads = nullptr, *adam_m = nullptr, *adam_v = nullptr;
     __nv_bfloat16 *wbf = nullptr;
+    // the forward's copy of the BF16 weights, [ci][tap][co] per layer (16-byte aligned
+    // layers): an input channel's weights for all output channels are contiguous
+    __nv_bfloat16 *wt = nullptr;
+    size_t wt_off[kLayers] = {};
+    size_t wt_total = 0;
     int step = 0;
     // activations for (aN, aH, aW)
     int aN = 0, aH = 0, aW = 0;
@@ -711,6 +744,19 @@ ConvIn conv_in(piv_net *n, const float *base, int i, int N)
     return c;
 }
 
+// the forward's weight copy from the FP32 masters (after every change of the weights)
+cudaError_t refresh_forward_weights(piv_net *n, cudaStream_t s)
+{
+    for (int i = 0; i < kLayers; ++i) {
+        const int cin = kSpec[i].ca + kSpec[i].cb, cout = kSpec[i].cout, nw = cout * cin * 9;
+        transpose_weights_kernel<<<(nw + 255) / 256, 256, 0, s>>>(n->params + n->w_off[i], cout, cin,
+                                                                  n->wt + n->wt_off[i]);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
 cudaError_t forward_layers(piv_net *n, float *act, int N, cudaStream_t s)
 {
     for (int i = 0; i < kLayers; ++i) {
@@ -722,7 +768,7 @@ cudaError_t forward_layers(piv_net *n, float *act, int N, cudaStream_t s)
         c.Ho = n->lh[lo];
         c.Wo = n->lw[lo];
         c.stride = sp.stride;
-        c.w = n->wbf + n->w_off[i];
+        c.w = n->wt + n->wt_off[i];
         c.bias = n->params + n->b_off[i];
         c.cout = sp.cout;
         c.out = act + n->t_off[i + 1];
@@ -829,6 +875,12 @@ int piv_net_create(uint64_t seed, piv_net **out)
         off += kSpec[i].cout;
     }
     n->n_params = off;
+    size_t woff = 0;
+    for (int i = 0; i < kLayers; ++i) {
+        n->wt_off[i] = woff;
+        woff += ((size_t)kSpec[i].cout * (kSpec[i].ca + kSpec[i].cb) * 9 + 7) & ~(size_t)7;  // 16-byte layers
+    }
+    n->wt_total = woff;
     // He-uniform weights for LeakyReLU (bound sqrt(6 / ((1 + slope^2) fan_in))), a head
     // scaled by 0.1, zero biases; Philox stream 4 of the seed
     std::vector<float> h(off, 0.f);
@@ -850,6 +902,7 @@ int piv_net_create(uint64_t seed, piv_net **out)
         cudaFree(n->adam_m);
         cudaFree(n->adam_v);
         cudaFree(n->wbf);
+        cudaFree(n->wt);
         cudaFree(n->d_loss);
         if (n->h_loss) cudaFreeHost(n->h_loss);
         if (n->stream) cudaStreamDestroy(n->stream);
@@ -861,6 +914,7 @@ int piv_net_create(uint64_t seed, piv_net **out)
         cudaMalloc(&n->adam_m, off * sizeof(float)) != cudaSuccess ||
         cudaMalloc(&n->adam_v, off * sizeof(float)) != cudaSuccess ||
         cudaMalloc(&n->wbf, off * sizeof(__nv_bfloat16)) != cudaSuccess ||
+        cudaMalloc(&n->wt, n->wt_total * sizeof(__nv_bfloat16)) != cudaSuccess ||
         cudaMalloc(&n->d_loss, sizeof(float)) != cudaSuccess ||
         cudaMallocHost(&n->h_loss, sizeof(float)) != cudaSuccess ||
         cudaStreamCreate(&n->stream) != cudaSuccess)  // blocking: ordered after default-stream work
@@ -871,7 +925,8 @@ int piv_net_create(uint64_t seed, piv_net **out)
         cudaMemset(n->grads, 0, off * sizeof(float)) != cudaSuccess)
         return fail(PIV_ERR_CUDA);
     to_bf16_kernel<<<(unsigned)((off + 255) / 256), 256, 0, n->stream>>>(n->params, n->wbf, off);
-    if (cudaStreamSynchronize(n->stream) != cudaSuccess) return fail(PIV_ERR_CUDA);
+    if (refresh_forward_weights(n, n->stream) != cudaSuccess || cudaStreamSynchronize(n->stream) != cudaSuccess)
+        return fail(PIV_ERR_CUDA);
     *out = n;
     return PIV_OK;
 }
@@ -886,6 +941,7 @@ int piv_net_destroy(piv_net *n)
     cudaFree(n->adam_m);
     cudaFree(n->adam_v);
     cudaFree(n->wbf);
+    cudaFree(n->wt);
     cudaFree(n->act);
     cudaFree(n->gact);
     cudaFree(n->din);
@@ -941,6 +997,7 @@ int piv_net_set_params(piv_net *n, const float *host, int64_t count)
     n->step = 0;
     to_bf16_kernel<<<(unsigned)((n->n_params + 255) / 256), 256, 0, n->stream>>>(n->params, n->wbf, n->n_params);
     NCK(cudaGetLastError());
+    NCK(refresh_forward_weights(n, n->stream));
     NCK(cudaStreamSynchronize(n->stream));
     return PIV_OK;
 }
@@ -1087,6 +1144,7 @@ int piv_net_adam_step(piv_net *n, float lr)
     adam_kernel<<<(unsigned)((n->n_params + 255) / 256), 256, 0, n->stream>>>(
         n->params, n->grads, n->adam_m, n->adam_v, n->wbf, n->n_params, lr, b1, b2, 1e-8f, c1, c2);
     NCK(cudaGetLastError());
+    NCK(refresh_forward_weights(n, n->stream));
     return PIV_OK;
 }
 
