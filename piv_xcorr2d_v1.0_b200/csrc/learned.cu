@@ -203,7 +203,9 @@ cudaError_t launch_features(const FeatArgs &a, cudaStream_t s)
         spread_y = std::max(spread_y, cv_centre(last, a.g.sp_y, a.g.Ny_left, a.g.ws_y) -
                                           cv_centre(iy0, a.g.sp_y, a.g.Ny_left, a.g.ws_y));
     }
-    const int LW = spread + Wd + 2 * kRadius, LHt = spread_y + Hd + 2 * kRadius;
+    // the region's row stride made odd: the threads of a warp read 9 shift rows of 4 vectors,
+    // which an even stride (144 floats at 64 px windows) put on 4 banks
+    const int LW = (spread + Wd + 2 * kRadius) | 1, LHt = spread_y + Hd + 2 * kRadius;
     const size_t smem = sizeof(float) * ((size_t)LHt * LW + (size_t)(LHt - 2 * kRadius) * (LW - 2 * kRadius));
     if (smem > 48 * 1024) return cudaErrorInvalidValue;
     const dim3 grid((a.g.Nx_vec + kCvVec - 1) / kCvVec, (a.g.Ny_vec + kCvRows - 1) / kCvRows);
@@ -233,6 +235,8 @@ struct ConvFwd {
     int cout;
     float *out;
     int act;
+    int splits;   // input-channel splits across CTAs (blockIdx.z = n * splits + split)
+    float *part;  // splits > 1: partial sums [N * splits][cout][Ho * Wo], finished by conv_finish_kernel
 };
 
 // tap offsets of output pixel (oy, ox): into a (upsampled or not) and into b
@@ -287,7 +291,7 @@ __global__ void __launch_bounds__(256) conv_fwd_kernel(const ConvFwd c)
     float(*wsm)[2][9][COT] = reinterpret_cast<float(*)[2][9][COT]>(csm);  // [warp][buffer][tap][co]
     float(*red)[COT][33] = reinterpret_cast<float(*)[COT][33]>(csm);      // [warp][co][pixel]
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int n = blockIdx.z, co0 = blockIdx.y * COT;
+    const int n = blockIdx.z / c.splits, split = blockIdx.z - n * c.splits, co0 = blockIdx.y * COT;
     const int HWo = c.Ho * c.Wo;
     const int p = blockIdx.x * 32 + lane;
     const bool live = p < HWo;
@@ -299,7 +303,7 @@ __global__ void __launch_bounds__(256) conv_fwd_kernel(const ConvFwd c)
 #pragma unroll
     for (int k = 0; k < COT; ++k) acc[k] = 0.f;
 #pragma unroll 1
-    for (int ci = warp; ci < cin; ci += 2 * NW) {
+    for (int ci = split * 2 * NW + warp; ci < cin; ci += 2 * NW * c.splits) {
         const int cj = ci + NW;
         const bool two = cj < cin;
         // both channels' weights: for each tap a contiguous run of COT output channels
@@ -354,12 +358,33 @@ __global__ void __launch_bounds__(256) conv_fwd_kernel(const ConvFwd c)
         const int k = e >> 5, l = e & 31;
         const int pp = blockIdx.x * 32 + l, co = co0 + k;
         if (pp >= HWo || co >= c.cout) continue;
-        float v = c.bias[co];
+        float v = 0.f;
 #pragma unroll
         for (int w = 0; w < NW; ++w) v += red[w][k][l];
+        if (c.splits > 1) {
+            c.part[((size_t)blockIdx.z * c.cout + co) * HWo + pp] = v;
+            continue;
+        }
+        v += c.bias[co];
         if (c.act) v = v > 0.f ? v : kSlope * v;
         c.out[((size_t)n * c.cout + co) * HWo + pp] = v;
     }
+}
+
+// bias + the splits' partial sums in split order + activation
+__global__ void conv_finish_kernel(const float *part, int splits, const float *bias, int N, int cout, int HWo, int act,
+                                   float *out)
+{
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (size_t)N * cout * HWo) return;
+    const int p = (int)(i % HWo);
+    const size_t r = i / HWo;
+    const int co = (int)(r % cout), n = (int)(r / cout);
+    float v = 0.f;
+    for (int sp = 0; sp < splits; ++sp) v += part[(((size_t)n * splits + sp) * cout + co) * HWo + p];
+    v += bias[co];
+    if (act) v = v > 0.f ? v : kSlope * v;
+    out[i] = v;
 }
 
 // dIn of the concatenated (upsampled) input, [N][ca+cb][Hin][Win], overwritten.
@@ -667,8 +692,9 @@ struct piv_net {
     int aN = 0, aH = 0, aW = 0;
     int lh[4] = {}, lw[4] = {};
     size_t t_off[kTensors] = {};
-    size_t act_floats = 0, din_floats = 0;
-    float *act = nullptr, *gact = nullptr, *din = nullptr;
+    size_t act_floats = 0, din_floats = 0, part_floats = 0;
+    float *act = nullptr, *gact = nullptr, *din = nullptr, *part = nullptr;
+    int splits[kLayers] = {};
     float *d_loss = nullptr, *h_loss = nullptr;
     // features scratch
     float *fdown = nullptr;
@@ -723,6 +749,21 @@ void layout(piv_net *n, int N, int H, int W)
         dmax = std::max(dmax, (size_t)N * (s.ca + s.cb) * n->lh[lin] * n->lw[lin]);
     }
     n->din_floats = dmax;
+    // input-channel splits of the forward convolutions: enough CTAs for two per SM, at
+    // least 16 input channels (two per warp) per split
+    size_t pmax = 0;
+    for (int i = 0; i < kLayers; ++i) {
+        const LayerSpec &s = kSpec[i];
+        const int lo = kLevel[i + 1], cin = s.ca + s.cb;
+        const int px = n->lh[lo] * n->lw[lo];
+        const long ctas = (long)((px + 31) / 32) * ((s.cout + 31) / 32) * N;
+        const int smax = std::max(1, cin / 16);
+        int sp = (int)std::min<long>(smax, std::max<long>(1, (2 * 148 + ctas - 1) / ctas));
+        if (s.cout % 32) sp = 1;
+        n->splits[i] = sp;
+        if (sp > 1) pmax = std::max(pmax, (size_t)N * sp * s.cout * px);
+    }
+    n->part_floats = pmax;
 }
 
 ConvIn conv_in(piv_net *n, const float *base, int i, int N)
@@ -773,14 +814,22 @@ cudaError_t forward_layers(piv_net *n, float *act, int N, cudaStream_t s)
         c.cout = sp.cout;
         c.out = act + n->t_off[i + 1];
         c.act = sp.act;
+        c.splits = n->splits[i];
+        c.part = n->part;
         const int px = c.Ho * c.Wo;
         if (sp.cout % 32 == 0) {
-            conv_fwd_kernel<32><<<dim3((px + 31) / 32, sp.cout / 32, N), 256, conv_fwd_smem<32>(), s>>>(c);
+            conv_fwd_kernel<32><<<dim3((px + 31) / 32, sp.cout / 32, N * c.splits), 256, conv_fwd_smem<32>(), s>>>(c);
         } else {
-            conv_fwd_kernel<2><<<dim3((px + 31) / 32, (sp.cout + 1) / 2, N), 256, conv_fwd_smem<2>(), s>>>(c);
+            conv_fwd_kernel<2><<<dim3((px + 31) / 32, (sp.cout + 1) / 2, N * c.splits), 256, conv_fwd_smem<2>(), s>>>(c);
         }
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
+        if (c.splits > 1) {
+            const size_t tot = (size_t)N * sp.cout * px;
+            conv_finish_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(n->part, c.splits, c.bias, N, sp.cout, px,
+                                                                            sp.act, c.out);
+            if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        }
     }
     return cudaSuccess;
 }
@@ -797,18 +846,22 @@ int net_reserve(piv_net *n, int N, int H, int W)
     cudaSetDevice(n->device);
     n->generation = next_generation();
     const size_t old_act = n->act ? n->act_floats : 0, old_din = n->act ? n->din_floats : 0;
+    const size_t old_part = n->act ? n->part_floats : 0;
     layout(n, N, H, W);
-    if (n->act_floats > old_act || n->din_floats > old_din || !n->act) {
+    if (n->act_floats > old_act || n->din_floats > old_din || n->part_floats > old_part || !n->act) {
         cudaFree(n->act);
         cudaFree(n->gact);
         cudaFree(n->din);
-        n->act = n->gact = n->din = nullptr;
+        cudaFree(n->part);
+        n->act = n->gact = n->din = n->part = nullptr;
         NCK(cudaMalloc(&n->act, n->act_floats * sizeof(float)));
         NCK(cudaMalloc(&n->gact, n->act_floats * sizeof(float)));
         NCK(cudaMalloc(&n->din, n->din_floats * sizeof(float)));
+        NCK(cudaMalloc(&n->part, std::max<size_t>(n->part_floats, 1) * sizeof(float)));
     } else {
         n->act_floats = std::max(n->act_floats, old_act);
         n->din_floats = std::max(n->din_floats, old_din);
+        n->part_floats = std::max(n->part_floats, old_part);
     }
     n->aN = N;
     n->aH = H;
@@ -945,6 +998,7 @@ int piv_net_destroy(piv_net *n)
     cudaFree(n->act);
     cudaFree(n->gact);
     cudaFree(n->din);
+    cudaFree(n->part);
     cudaFree(n->d_loss);
     cudaFree(n->fdown);
     cudaFree(n->fsums);
