@@ -316,13 +316,11 @@ __global__ void __launch_bounds__(256) conv_fwd_kernel(const ConvFwd c)
                 if (ch == 0 || two)
                     u = __ldg(reinterpret_cast<const uint4 *>(c.w + ((size_t)cc * 9 + tap) * c.cout + co0) + q);
                 const __nv_bfloat162 *h = reinterpret_cast<const __nv_bfloat162 *>(&u);
-                float *dst = &wsm[warp][ch][tap][8 * q];
-#pragma unroll
-                for (int j = 0; j < 4; ++j) {
-                    const float2 f = __bfloat1622float2(h[j]);
-                    dst[2 * j] = f.x;
-                    dst[2 * j + 1] = f.y;
-                }
+                const float2 f0 = __bfloat1622float2(h[0]), f1 = __bfloat1622float2(h[1]);
+                const float2 f2 = __bfloat1622float2(h[2]), f3 = __bfloat1622float2(h[3]);
+                float4 *dst = reinterpret_cast<float4 *>(&wsm[warp][ch][tap][8 * q]);  // 16-byte stores
+                dst[0] = make_float4(f0.x, f0.y, f1.x, f1.y);
+                dst[1] = make_float4(f2.x, f2.y, f3.x, f3.y);
             }
         } else {
             for (int e = lane; e < 2 * 9 * COT; e += 32) {
