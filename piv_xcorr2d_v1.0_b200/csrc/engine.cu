@@ -1098,6 +1098,7 @@ int piv_run_pair_learned(piv_engine *e, piv_net *n, float max_reject_frac, float
     CK(cudaGraphLaunch(e->learned_exec, e->stream));
     CK(cudaMemcpyAsync(e->h_judge, e->d_judge, 2 * sizeof(float), cudaMemcpyDeviceToHost, e->stream));
     CK(cudaStreamSynchronize(e->stream));
+    if ((rc = learned::net_check_status(n))) return set_err(e, rc, "predictor network: tensor-core wait timed out");
     const float rej = e->h_judge[1] / (float)g2.gg.Nt_vec;
     const float rms = std::sqrt(e->h_judge[0] / (float)g2.gg.Nt_vec);
     if (reject_frac) *reject_frac = rej;

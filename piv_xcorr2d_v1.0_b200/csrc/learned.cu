@@ -12,11 +12,13 @@
 #include <atomic>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
 
 #include "learned.cuh"
+#include "tc_common.cuh"
 #include "piv_b200.h"
 #include "synth_model.h"
 
@@ -385,6 +387,201 @@ __global__ void conv_finish_kernel(const float *part, int splits, const float *b
     out[i] = v;
 }
 
+// Forward convolution on the tensor cores, for stride-1 layers with 32 or 64 output
+// channels over enough pixels: an implicit GEMM D[pixel][co] = sum_k A[pixel][k] W[co][k],
+// k = (input channel, tap), on tcgen05 (kind::f16, FP32 accumulation in tensor memory).
+//   - A CTA takes an 8 x 16 tile of output pixels (M = 128) with 512 threads, four per
+//     pixel (a CTA holding tensor memory is resident once per SM, and 4 warps per SM left
+//     every dependent instruction exposed).  Per block of 16 input channels it stages the
+//     10 x 18 input patch (FP32, zero padded, through the upsampling / concatenation of the
+//     layer's input) in shared memory and builds all 9 taps' operands from it: each thread
+//     writes 4 of its pixel's 16 channel values as BF16 hi + lo pairs (x ~= hi + lo, about
+//     16 significant bits) into the K-major A operand of each tap, and the threads copy
+//     each tap's 16 x N weights ([ci][tap][co], BF16, exact) as the MN-major B operand.  After one barrier thread 0 issues the
+//     block's 18 MMAs (D += A_hi W + A_lo W per tap) and one commit.
+//   - Blocks alternate between two operand buffers: the tensor core works on block b while
+//     the threads stage block b + 1.  The commit of block b - 2 on the buffer's mbarrier
+//     frees it; every wait is bounded (kMaxTries probes), and a timeout sets bit 0 of
+//     *status, skips the epilogue and still releases the tensor memory.
+//   - Epilogue: warp w reads the accumulators of pixels 32 (w % 4) .. + 31 (its lane
+//     quarter of tensor memory), 16 output channels per warpgroup (tcgen05.ld), adds the
+//     bias, applies LeakyReLU and stores.
+constexpr int kTcTY = 8, kTcTX = 16, kTcPY = kTcTY + 2, kTcPX = kTcTX + 2, kTcCB = 16;
+
+template <int N>
+struct ConvTcSmem {
+    float patch[2][kTcCB][kTcPY][kTcPX];
+    alignas(128) uint8_t a_hi[2][9][128 * kTcCB * 2];
+    alignas(128) uint8_t a_lo[2][9][128 * kTcCB * 2];
+    alignas(128) uint8_t b[2][9][N * kTcCB * 2];
+    alignas(8) uint64_t mbar[3];
+    uint32_t tmem_base;
+};
+
+// cp.async of one float into shared memory; zero-filled (nothing read) when !valid
+__device__ __forceinline__ void cp_async_f32(uint32_t dst, const float *src, bool valid)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(dst), "l"(src), "r"(valid ? 4 : 0) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int PENDING>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(PENDING) : "memory"); }
+
+// the input patch of channel block `blk` into `patch` by cp.async (one group per call):
+// threads 0..359 each own one of the 180 patch positions for 8 of the 16 channels, so the
+// position's bounds and offsets are worked out once (the channels are a plane apart)
+__device__ __forceinline__ void conv_tc_patch(const ConvFwd &c, int n, int x0, int y0, int blk, int tid,
+                                              float (*patch)[kTcPY][kTcPX])
+{
+    constexpr int NPOS = kTcPY * kTcPX;
+    if (tid < 2 * NPOS) {
+        const int pos = tid < NPOS ? tid : tid - NPOS, ch0 = tid < NPOS ? 0 : kTcCB / 2;
+        const int py = pos / kTcPX, px = pos - py * kTcPX;
+        const int y = y0 - 1 + py, x = x0 - 1 + px;
+        const bool inside = y >= 0 && y < c.in.Hin && x >= 0 && x < c.in.Win;
+        const int cin = c.in.ca + c.in.cb, cb0 = blk * kTcCB + ch0;
+        const size_t plane_a = (size_t)c.in.Ha * c.in.Wa, plane_b = (size_t)c.in.Hin * c.in.Win;
+        const int off_a = inside ? (c.in.up ? (y >> 1) * c.in.Wa + (x >> 1) : y * c.in.Win + x) : 0;
+        const int off_b = inside ? y * c.in.Win + x : 0;
+        const uint32_t dst = tc::smem_u32(&patch[ch0][py][px]);
+#pragma unroll
+        for (int q = 0; q < kTcCB / 2; ++q) {
+            const int cc = cb0 + q;
+            const bool ok = inside && cc < cin;
+            const float *src = c.in.a;  // any valid address where nothing is read
+            if (ok)
+                src = cc < c.in.ca ? c.in.a + ((size_t)n * c.in.ca + cc) * plane_a + off_a
+                                   : c.in.b + ((size_t)n * c.in.cb + (cc - c.in.ca)) * plane_b + off_b;
+            cp_async_f32(dst + (uint32_t)(q * NPOS * 4), src, ok);
+        }
+    }
+    cp_async_commit();
+}
+
+template <int N>
+__global__ void __launch_bounds__(512, 1) conv_tc_kernel(const ConvFwd c, int *status)
+{
+    extern __shared__ __align__(128) uint8_t tc_raw[];
+    ConvTcSmem<N> &S = *reinterpret_cast<ConvTcSmem<N> *>(tc_raw);
+    constexpr uint32_t TCOLS = N < 32 ? 32 : N;
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const int n = blockIdx.z, x0 = blockIdx.x * kTcTX, y0 = blockIdx.y * kTcTY;
+    const int px_id = tid >> 2, quarter = tid & 3;  // the pixel (A row) and the 4 channels this thread builds
+    const int ty = px_id >> 4, tx = px_id & 15;
+    const int cin = c.in.ca + c.in.cb, nblk = (cin + kTcCB - 1) / kTcCB;
+    if (tid == 0) {
+        for (int i = 0; i < 3; ++i) tc::mbar_init(tc::smem_u32(&S.mbar[i]), 1);
+        tc::fence_mbar_init();
+    }
+    if (warp == 0) tc::tmem_alloc(tc::smem_u32(&S.tmem_base), TCOLS);
+    conv_tc_patch(c, n, x0, y0, 0, tid, S.patch[0]);
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = S.tmem_base;
+    constexpr uint32_t idesc = tc::idesc_f16(N, false, true, true);
+    // K-major A: byte (k/8)*2048 + m*16 + (k%8)*2 with m = px_id; this thread's channels
+    // k = 4*quarter .. + 3 are 8 bytes at (quarter/2)*2048 + m*16 + (quarter%2)*8
+    const uint32_t a_off = (uint32_t)(quarter >> 1) * 2048u + (uint32_t)px_id * 16u + (uint32_t)(quarter & 1) * 8u;
+    bool ok = true;
+    int blk = 0;
+    for (; blk < nblk; ++blk) {
+        const int bb = blk & 1, cb0 = blk * kTcCB;
+        // the next block's patch streams in while this one is built (its buffer was last
+        // read by block blk - 1's operand build, finished before that block's MMA barrier)
+        if (blk + 1 < nblk) {
+            conv_tc_patch(c, n, x0, y0, blk + 1, tid, S.patch[bb ^ 1]);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        if (blk >= 2) {
+            // the MMAs of block blk - 2 read this block's operand buffers: wait for their commit
+            const bool done = tc::mbar_wait(tc::smem_u32(&S.mbar[bb]), ((blk >> 1) - 1) & 1);
+            if (!__syncthreads_and(done)) {
+                ok = false;
+                break;
+            }
+            tc::fence_after_sync();
+        } else {
+            __syncthreads();  // every thread's patch copies have landed
+        }
+        float(*patch)[kTcPY][kTcPX] = S.patch[bb];
+        // the weights of the block's 9 taps: chunk (tap, g = co/8, k) at byte (co/8)*256 + k*16
+        for (int e = tid; e < 9 * 2 * N; e += 512) {
+            const int tap = e / (2 * N), r = e - tap * (2 * N), g = r / kTcCB, k = r - g * kTcCB, cc = cb0 + k;
+            uint4 w = make_uint4(0u, 0u, 0u, 0u);
+            if (cc < cin) w = __ldg(reinterpret_cast<const uint4 *>(c.w + ((size_t)cc * 9 + tap) * c.cout) + g);
+            reinterpret_cast<uint4 *>(S.b[bb][tap])[g * kTcCB + k] = w;
+        }
+#pragma unroll 1
+        for (int tap = 0; tap < 9; ++tap) {
+            const int ky = tap / 3, kx = tap - ky * 3;
+            uint32_t hi[2], lo[2];
+#pragma unroll
+            for (int j = 0; j < 2; ++j) {
+                const int k = 4 * quarter + 2 * j;
+                tc::split_bf16x2(patch[k][ty + ky][tx + kx], patch[k + 1][ty + ky][tx + kx], hi[j], lo[j]);
+            }
+            *reinterpret_cast<uint2 *>(S.a_hi[bb][tap] + a_off) = make_uint2(hi[0], hi[1]);
+            *reinterpret_cast<uint2 *>(S.a_lo[bb][tap] + a_off) = make_uint2(lo[0], lo[1]);
+        }
+        tc::fence_async_smem();
+        tc::fence_before_sync();
+        __syncthreads();
+        if (tid == 0) {
+            tc::fence_after_sync();
+            for (int tap = 0; tap < 9; ++tap) {
+                const uint64_t bd = tc::smem_desc(tc::smem_u32(S.b[bb][tap]), 128, 256);
+                tc::mma_f16(tmem, tc::smem_desc(tc::smem_u32(S.a_hi[bb][tap]), 2048, 128), bd, idesc,
+                            (blk > 0 || tap > 0) ? 1u : 0u);
+                tc::mma_f16(tmem, tc::smem_desc(tc::smem_u32(S.a_lo[bb][tap]), 2048, 128), bd, idesc, 1u);
+            }
+            tc::mma_commit(tc::smem_u32(&S.mbar[bb]));
+        }
+    }
+    cp_async_wait<0>();  // no copy outlives the CTA (the early exit leaves one in flight)
+    if (tid == 0 && ok) tc::mma_commit(tc::smem_u32(&S.mbar[2]));
+    const bool fin = ok && __syncthreads_and(tc::mbar_wait(tc::smem_u32(&S.mbar[2]), 0));
+    if (!fin) {
+        if (tid == 0 && status) atomicOr(status, 1);
+        // the block in flight gets one more bounded wait before the tensor memory is released
+        if (blk > 0) tc::mbar_wait(tc::smem_u32(&S.mbar[(blk - 1) & 1]), ((blk - 1) >> 1) & 1);
+    } else if (warp / 4 < N / 16) {
+        tc::fence_after_sync();
+        const int lq = warp & 3, c0 = (warp >> 2) * 16;   // lane quarter, 16 output channels
+        const int pe = lq * 32 + (tid & 31);              // this thread's pixel in the epilogue
+        const int y = y0 + (pe >> 4), x = x0 + (pe & 15);
+        const bool live = y < c.Ho && x < c.Wo;
+        const int HWo = c.Ho * c.Wo;
+        float v[16];
+        tc::tmem_ld16(tmem + ((uint32_t)(lq * 32) << 16) + c0, v);
+        tc::tmem_wait_ld();
+        if (live) {
+#pragma unroll
+            for (int k = 0; k < 16; ++k) {
+                float o = v[k] + c.bias[c0 + k];
+                if (c.act) o = o > 0.f ? o : kSlope * o;
+                c.out[((size_t)n * c.cout + c0 + k) * HWo + y * c.Wo + x] = o;
+            }
+        }
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) tc::tmem_dealloc(tmem, TCOLS);
+}
+
+template <int N>
+cudaError_t launch_conv_tc(const ConvFwd &c, int *status, cudaStream_t s)
+{
+    const size_t smem = sizeof(ConvTcSmem<N>);
+    cudaError_t e = cudaFuncSetAttribute(conv_tc_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    const dim3 grid((c.Wo + kTcTX - 1) / kTcTX, (c.Ho + kTcTY - 1) / kTcTY, c.N);
+    conv_tc_kernel<N><<<grid, 512, smem, s>>>(c, status);
+    return cudaGetLastError();
+}
+
 // dIn of the concatenated (upsampled) input, [N][ca+cb][Hin][Win], overwritten.
 struct ConvBwdData {
     int N, cin, Hin, Win, Ho, Wo, stride, cout;
@@ -700,6 +897,8 @@ struct piv_net {
     size_t fcap = 0;
     cudaStream_t stream = nullptr;
     std::string err;
+    int *d_status = nullptr;  // bit 0: a tensor-core convolution's MMA wait timed out
+    bool use_tc = true;       // tensor-core forward for the wide stride-1 layers (PIV_NET_TC=0: off)
     // drawn from a process-wide counter at creation and whenever a buffer a captured graph
     // may hold is reallocated or re-laid-out, so (net, generation) never repeats
     unsigned generation = 0;
@@ -815,6 +1014,11 @@ cudaError_t forward_layers(piv_net *n, float *act, int N, cudaStream_t s)
         c.splits = n->splits[i];
         c.part = n->part;
         const int px = c.Ho * c.Wo;
+        if (n->use_tc && sp.stride == 1 && (sp.cout == 32 || sp.cout == 64) && (long)N * px >= 4096) {
+            cudaError_t e = sp.cout == 32 ? launch_conv_tc<32>(c, n->d_status, s) : launch_conv_tc<64>(c, n->d_status, s);
+            if (e != cudaSuccess) return e;
+            continue;
+        }
         if (sp.cout % 32 == 0) {
             conv_fwd_kernel<32><<<dim3((px + 31) / 32, sp.cout / 32, N * c.splits), 256, conv_fwd_smem<32>(), s>>>(c);
         } else {
@@ -900,6 +1104,16 @@ int net_reserve_features(piv_net *n, int Nx, int Ny)
 }
 
 unsigned net_generation(const piv_net *n) { return n->generation; }
+
+int net_check_status(piv_net *n)
+{
+    int st = 0;
+    if (cudaMemcpy(&st, n->d_status, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return PIV_ERR_CUDA;
+    if (!st) return PIV_OK;
+    cudaMemset(n->d_status, 0, sizeof(int));
+    n->err = "a tensor-core convolution's MMA completion wait timed out";
+    return PIV_ERR_DEVICE;
+}
 float *net_feature_down(piv_net *n) { return n->fdown; }
 double *net_feature_sums(piv_net *n) { return n->fsums; }
 
@@ -955,6 +1169,7 @@ int piv_net_create(uint64_t seed, piv_net **out)
         cudaFree(n->wbf);
         cudaFree(n->wt);
         cudaFree(n->d_loss);
+        cudaFree(n->d_status);
         if (n->h_loss) cudaFreeHost(n->h_loss);
         if (n->stream) cudaStreamDestroy(n->stream);
         delete n;
@@ -967,14 +1182,17 @@ int piv_net_create(uint64_t seed, piv_net **out)
         cudaMalloc(&n->wbf, off * sizeof(__nv_bfloat16)) != cudaSuccess ||
         cudaMalloc(&n->wt, n->wt_total * sizeof(__nv_bfloat16)) != cudaSuccess ||
         cudaMalloc(&n->d_loss, sizeof(float)) != cudaSuccess ||
+        cudaMalloc(&n->d_status, sizeof(int)) != cudaSuccess ||
         cudaMallocHost(&n->h_loss, sizeof(float)) != cudaSuccess ||
         cudaStreamCreate(&n->stream) != cudaSuccess)  // blocking: ordered after default-stream work
         return fail(PIV_ERR_CUDA);
     if (cudaMemcpy(n->params, h.data(), off * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemset(n->adam_m, 0, off * sizeof(float)) != cudaSuccess ||
         cudaMemset(n->adam_v, 0, off * sizeof(float)) != cudaSuccess ||
-        cudaMemset(n->grads, 0, off * sizeof(float)) != cudaSuccess)
+        cudaMemset(n->grads, 0, off * sizeof(float)) != cudaSuccess ||
+        cudaMemset(n->d_status, 0, sizeof(int)) != cudaSuccess)
         return fail(PIV_ERR_CUDA);
+    if (const char *tc = getenv("PIV_NET_TC")) n->use_tc = tc[0] != '0';
     to_bf16_kernel<<<(unsigned)((off + 255) / 256), 256, 0, n->stream>>>(n->params, n->wbf, off);
     if (refresh_forward_weights(n, n->stream) != cudaSuccess || cudaStreamSynchronize(n->stream) != cudaSuccess)
         return fail(PIV_ERR_CUDA);
@@ -998,6 +1216,7 @@ int piv_net_destroy(piv_net *n)
     cudaFree(n->din);
     cudaFree(n->part);
     cudaFree(n->d_loss);
+    cudaFree(n->d_status);
     cudaFree(n->fdown);
     cudaFree(n->fsums);
     if (n->h_loss) cudaFreeHost(n->h_loss);
@@ -1205,7 +1424,7 @@ int piv_net_synchronize(piv_net *n)
     if (!n) return PIV_ERR_ARG;
     cudaSetDevice(n->device);
     NCK(cudaStreamSynchronize(n->stream));
-    return PIV_OK;
+    return net_check_status(n);
 }
 
 }  // extern "C"

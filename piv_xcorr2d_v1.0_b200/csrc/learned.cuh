@@ -56,6 +56,9 @@ cudaError_t launch_judge(const float *px, const float *py, const float *fx, cons
 // changes whenever net_reserve / net_reserve_features move or re-lay-out a buffer: a
 // graph captured with the net's buffers is stale once it differs
 unsigned net_generation(const piv_net *n);
+// PIV_ERR_DEVICE (and clears it) if a tensor-core convolution reported a timed-out wait;
+// synchronous (reads one word)
+int net_check_status(piv_net *n);
 // feature scratch owned by the net (sized for the largest frame seen)
 int net_reserve_features(piv_net *n, int Nx, int Ny);
 float *net_feature_down(piv_net *n);

@@ -98,6 +98,51 @@ def test_forward_loss_and_gradient_match_oracle(cuda, shape):
             assert err < 2e-4, (i, lo == b_off, err)
 
 
+def test_tensor_core_forward_matches_oracle_and_simt(cuda, monkeypatch):
+    """At 130 x 132 the wide stride-1 layers (0, 1 and 11 with 32 output channels, 3 and 10
+    with 64, the last two through upsampling and concatenation) run on the tcgen05
+    convolution, with partial tiles at both edges: its forward output, the loss and the
+    gradients match the oracle, and its output matches the SIMT kernels'."""
+    import torch
+
+    N, H, W = 1, 130, 132
+    x, label, mask = _batch(21, N, H, W)
+    dx = torch.from_numpy(x).cuda()
+    dl = torch.from_numpy(label).cuda()
+    dm = torch.from_numpy(mask).cuda()
+    outs = {}
+    for tc in ("1", "0"):
+        monkeypatch.setenv("PIV_NET_TC", tc)
+        with P.PredictorNet(seed=6) as net:
+            params = net.params()
+            rng = np.random.default_rng(2)
+            for (w_off, b_off, cout, cin) in L.layout()[0]:
+                params[b_off: b_off + cout] = rng.normal(0, 0.05, cout)
+            net.set_params(params)
+            out = torch.empty((N, 2, H, W), dtype=torch.float32, device="cuda")
+            net.forward(dx, N, H, W, out)
+            net.synchronize()
+            outs[tc] = out.cpu().numpy()
+            if tc == "1":
+                loss = net.loss_grad(dx, dl, dm, N, H, W)
+                grad = net.grads()
+    want_loss, want_grad, want_out = L.loss_and_grad(params.astype(np.float64), x.astype(np.float64),
+                                                    label.astype(np.float64), mask.astype(np.float64))
+    scale = 1 + np.abs(want_out).max()
+    assert np.abs(outs["1"] - want_out).max() <= 1e-4 * scale
+    assert np.abs(outs["1"] - outs["0"]).max() <= 1e-4 * scale
+    assert abs(loss - want_loss) <= 1e-5 * (1 + abs(want_loss))
+    # the backward kernels read the tensor-core forward's activations (split-BF16 operands,
+    # about 1e-5 relative): the few pre-activations within that of zero take the other side
+    # of the LeakyReLU kink, which moves the 17k-pixel gradient sums of the layers computed
+    # on the tensor cores by up to about 1e-3 relative (SIMT forward: 1e-6, the bar above)
+    for i, (w_off, b_off, cout, cin) in enumerate(L.layout()[0]):
+        for lo, hi in ((w_off, b_off), (b_off, b_off + cout)):
+            g, w = grad[lo:hi], want_grad[lo:hi]
+            err = np.linalg.norm(g - w) / max(np.linalg.norm(w), 1e-12)
+            assert err < 3e-3, (i, lo == b_off, err)
+
+
 def test_adam_step(cuda):
     import torch
 
