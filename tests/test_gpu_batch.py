@@ -85,3 +85,29 @@ def test_batch_rejects_mixed_pass_counts(cuda):
     c.Npass2 = 2
     with pytest.raises(P.PivError):
         P.Batch([a, c])
+
+
+def test_batch_group_over_96_pairs_single_grid(cuda):
+    """100 pairs of one window shape form one group, which takes two launches (96 + 4 pairs
+    per launch parameter); grid 1 only (Npass2 = 0).  Every pair matches its run alone."""
+    n = 100
+    p = P.default_params(Nx=160, Ny=128, if_mhe=0, ws_x1=32, ws_y1=32, spacing_x1=16, spacing_y1=16, Npass1=2,
+                         ws_x2=32, ws_y2=32, spacing_x2=16, spacing_y2=16, Npass2=0)
+    frames = []
+    for k in range(n):
+        s = P.synth_params(160, 128, ppp=0.05, field=P.PIV_FIELD_UNIFORM, a=1.0 + 0.02 * k, b=-0.5, seed=900 + k)
+        frames.append(P.synth_pair(s))
+    with P.Batch([p] * n) as b:
+        groups = b.groups()
+        assert [g["pairs"] for g in groups] == [n, n]  # grid 1: the undeformed and the deformed pass
+        for e, (f1, f2) in zip(b.engines, frames):
+            e.set_images(f1, f2)
+        b.run()
+        b.synchronize()
+        got = [b.engines[i].field(1) for i in (0, 95, 96, 99)]
+    for i, g in zip((0, 95, 96, 99), got):
+        with P.Engine(p) as e:
+            e.set_images(*frames[i])
+            e.run_pair()
+            for u, v in zip(g, e.field(1)):
+                assert np.array_equal(u, v), i
