@@ -257,3 +257,35 @@ def test_trained_predictor_gain(cuda):
         print(f"grid 2 vs truth: plain {acc_plain:.4f} px, learned {acc_learned:.4f} px, judge {r}")
         assert not r["fell_back"]
         assert acc_learned <= acc_plain + 0.01
+
+
+def test_learned_pair_tensor_core_layers(cuda, monkeypatch):
+    """At 4096 x 2160 the grid-1 vector grid (127 x 67) is large enough for the predictor's
+    level-0 convolutions to run on the tensor cores inside the learned pair's graph: the
+    pair passes the judge with them on and off, and the final grid-2 fields agree to a
+    small fraction of a pixel (the split-BF16 activations move the prediction by ~1e-5
+    relative; the grid-2 passes then converge on the same peaks)."""
+    assert WEIGHTS.exists()
+    Nx, Ny = 4096, 2160
+    s = P.synth_params(Nx, Ny, ppp=0.04, field=P.PIV_FIELD_FOURIER, a=300.0, b=2000.0, c=8.0, seed=777)
+    f1, f2 = P.synth_pair(s)
+    p = P.default_params(Nx=Nx, Ny=Ny, if_mhe=1, mhe_ws=40, mhe_thresh=0.91, ws_x1=64, ws_y1=64, spacing_x1=32,
+                         spacing_y1=32, Npass1=2, ws_x2=32, ws_y2=32, spacing_x2=16, spacing_y2=16, Npass2=3,
+                         insert_threshold_p1=2.0, insert_threshold_p2=2.0)
+    fields = {}
+    for tc in ("1", "0"):
+        monkeypatch.setenv("PIV_NET_TC", tc)
+        with P.Engine(p) as e, P.PredictorNet(weights=WEIGHTS) as net:
+            assert e.geom["Ny_vec"][0] * e.geom["Nx_vec"][0] >= 4096
+            e.set_images(f1, f2)
+            r = e.run_pair_learned(net)
+            assert not r["fell_back"], r
+            fields[tc] = e.field(3)
+    x, y, dx1, dy1, v1 = fields["1"]
+    _, _, dx0, dy0, v0 = fields["0"]
+    both = (v1 == 1) & (v0 == 1)
+    assert both.mean() > 0.99
+    d = np.hypot(dx1 - dx0, dy1 - dy0)[both]
+    assert np.quantile(d, 0.999) < 0.01 and d.max() < 0.5
+    u, w = P.synth_field(s, x, y)
+    assert np.sqrt(np.mean(((dx1 - u) ** 2 + (dy1 - w) ** 2)[v1 == 1])) < 0.1
