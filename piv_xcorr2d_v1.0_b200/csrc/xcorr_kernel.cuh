@@ -226,45 +226,60 @@ __device__ __forceinline__ void peak_select(int Nps, int lane, float (&tv)[K], i
     }
 }
 
-// Sub-pixel fit of the candidate held by lane (< Nps), limits, NaN/Inf removal and the
-// stores of the window's outputs; cnt is the window's count of maxima.
+// Sub-pixel fit of the candidates held by lanes < Nps, limits, NaN/Inf removal and the
+// stores of the window's outputs; cnt is the window's count of maxima.  Called by whole
+// warps (the fits' x and y halves run on separate lanes and meet by shuffle).
 template <int WSX, int WSY>
 __device__ __forceinline__ void peak_fit_store(const XcorrArgs &a, const float *P, int w, int lane, float v, int idx,
                                                int cnt, float pred_x, float pred_y)
 {
     constexpr int LDF = WSX + 1;
     const GridGeom &g = a.g;
-    if (lane < g.Nps) {
+    const int Nps = g.Nps;
+    // lanes [0, Nps) fit x and lanes [Nps, 2 Nps) fit y of the same candidates (the fits are
+    // independent, so each lane does one instead of two: the warp issues the FP64 path once)
+    const int comp = lane < Nps ? 0 : (lane < 2 * Nps ? 1 : 2);
+    const int k = comp == 1 ? lane - Nps : lane;
+    const float cv = __shfl_sync(0xffffffffu, v, k & 31);
+    const int cidx = __shfl_sync(0xffffffffu, idx, k & 31);
+    float sh = 0.f;
+    bool inner = false;
+    if (comp < 2 && cv > 0.f) {
+        const int j = cidx / WSX, i = cidx - j * WSX;
+        if (i != 0 && i != WSX - 1 && j != 0 && j != WSY - 1) {
+            const float *pc = P + j * LDF + i;
+            const int step = comp ? LDF : 1;
+            const float f0 = pc[-step], f2 = pc[step];
+            const double dv = (double)cv * (double)cv;
+            // numerator ln f- - ln f+ in FP32 as the reference; the cancelling
+            // denominator ln(f- f+ / f0^2) in FP64
+            const float nn = logf(f0) - logf(f2);
+            const double den = log(((double)f0 * (double)f2) / dv);
+            sh = (float)((double)nn / den / 2.0);
+            inner = true;
+        }
+    }
+    const float sy = __shfl_sync(0xffffffffu, sh, (lane + Nps) & 31);
+    if (lane < Nps) {
         float ox = 0.f, oy = 0.f;
         bool ok = false;
-        if (v > 0.f) {
+        if (inner) {
             const int j = idx / WSX, i = idx - j * WSX;
-            if (i != 0 && i != WSX - 1 && j != 0 && j != WSY - 1) {
-                const float *pc = P + j * LDF + i;
-                const float c0 = pc[-1], c2 = pc[1], d0 = pc[-LDF], d2 = pc[LDF];
-                const double dv = (double)v * (double)v;
-                // numerator ln f- - ln f+ in FP32 as the reference; the cancelling
-                // denominator ln(f- f+ / f0^2) in FP64
-                const float nx = logf(c0) - logf(c2), ny = logf(d0) - logf(d2);
-                const double denx = log(((double)c0 * (double)c2) / dv);
-                const double deny = log(((double)d0 * (double)d2) / dv);
-                const float sx = (float)((double)nx / denx / 2.0), sy = (float)((double)ny / deny / 2.0);
-                ox = (float)i + sx - (float)WSX / 2 + pred_x;
-                oy = (float)j + sy - (float)WSY / 2 + pred_y;
-                ok = true;
-                if (ox < g.lx1 || ox > g.lx2 || oy < g.ly1 || oy > g.ly2) {
-                    ok = false;
-                    ox = 0.f;
-                    oy = 0.f;
-                }
-                if (isnan(ox) || isnan(oy) || isinf(ox) || isinf(oy)) {
-                    ok = false;
-                    ox = 0.f;
-                    oy = 0.f;
-                }
+            ox = (float)i + sh - (float)WSX / 2 + pred_x;
+            oy = (float)j + sy - (float)WSY / 2 + pred_y;
+            ok = true;
+            if (ox < g.lx1 || ox > g.lx2 || oy < g.ly1 || oy > g.ly2) {
+                ok = false;
+                ox = 0.f;
+                oy = 0.f;
+            }
+            if (isnan(ox) || isnan(oy) || isinf(ox) || isinf(oy)) {
+                ok = false;
+                ox = 0.f;
+                oy = 0.f;
             }
         }
-        const size_t o = (size_t)w * g.Nps + lane;
+        const size_t o = (size_t)w * Nps + lane;
         a.cdx[o] = ox;
         a.cdy[o] = oy;
         a.cvalid[o] = ok ? 1 : 0;
