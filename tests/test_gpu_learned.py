@@ -55,6 +55,30 @@ def test_features_match_oracle(cuda):
     assert (np.abs(k // 9 - 4) <= 2).all() and (np.abs(k % 9 - 4) <= 2).all()
 
 
+@pytest.mark.parametrize("ws,sp", [(32, 16), (48, 24)])
+def test_features_other_window_sizes(cuda, ws, sp):
+    """The cost volume's generic window width (ws/4 = 8 and 12 downsampled px) against the
+    oracle."""
+    import torch
+
+    Nx, Ny = 400, 336
+    s = P.synth_params(Nx, Ny, ppp=0.05, field=P.PIV_FIELD_VORTEX, a=4.0, b=100.0, c=0.0, seed=6)
+    f1, f2 = P.synth_pair(s)
+    p = P.default_params(Nx=Nx, Ny=Ny, if_mhe=0, ws_x1=ws, ws_y1=ws, spacing_x1=sp, spacing_y1=sp, Npass1=1,
+                         ws_x2=32, ws_y2=32, spacing_x2=16, spacing_y2=16, Npass2=0)
+    with P.Engine(p) as e, P.PredictorNet(seed=1) as net:
+        e.set_images(f1, f2)
+        e.prep()
+        g = e.geom
+        H, W = g["Ny_vec"][0], g["Nx_vec"][0]
+        out = torch.empty(81 * H * W, dtype=torch.float32, device="cuda")
+        e.features(net, out)
+        e.synchronize()
+        got = out.cpu().numpy().reshape(81, H, W)
+    want = L.features(f1, f2, W, H, sp, sp, g["Nx_left"][0], g["Ny_left"][0], ws, ws)
+    assert np.abs(got - want).max() < 2e-5
+
+
 def _batch(seed, N, H, W):
     rng = np.random.default_rng(seed)
     x = rng.normal(0, 0.5, (N, 81, H, W)).astype(np.float32)
