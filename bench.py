@@ -61,19 +61,41 @@ def load_pkg():
     return mod
 
 
+# Every value of the parameter file (X/Parameter.dat order) for the workload; both arms
+# take their parameters from this one table.
+WORKLOAD = dict(
+    device_id=0, if_mhe=1, mhe_ws=40, mhe_thresh=0.91, Nx=NX, Ny=NY,
+    ws_x1=64, ws_y1=64, spacing_x1=32, spacing_y1=32, Npass1=2,
+    ws_x2=32, ws_y2=32, spacing_x2=16, spacing_y2=16, Npass2=3, Nsec_cc=1,
+    wx1_median=5, wy1_median=5, Npass1_median=2, minNneigh_p1=5, residual_threshold_p1=2.0, insert_threshold_p1=2.0,
+    wx1_smooth=3, wy1_smooth=3, Npass1_smooth=1,
+    wx2_median=5, wy2_median=5, Npass2_median=2, minNneigh_p2=5, residual_threshold_p2=2.0, insert_threshold_p2=2.0,
+    wx2_smooth=3, wy2_smooth=3, Npass2_smooth=1,
+    max_dispx_win_percent1=0.4, max_dispy_win_percent1=0.4, max_dispx_win_percent2=0.4, max_dispy_win_percent2=0.4,
+    Npeak_save=4, dispx_lim1=-100.0, dispx_lim2=100.0, dispy_lim1=-100.0, dispy_lim2=100.0)
+# The seeded pair: 0.04 particles/px, sigma 0.6 px, Lamb-Oseen vortex (10 px, 600 px core) + 0.002 shear.
+SYNTH = dict(ppp=0.04, sigma=0.6, field=1, a=10.0, b=600.0, c=0.002)
+
+
 def workload_params(P, device_id=0, Ny=NY):
-    return P.default_params(device_id=device_id, Nx=NX, Ny=Ny, if_mhe=1, mhe_ws=40, mhe_thresh=0.91,
-                            ws_x1=64, ws_y1=64, spacing_x1=32, spacing_y1=32, Npass1=2,
-                            ws_x2=32, ws_y2=32, spacing_x2=16, spacing_y2=16, Npass2=3, Nsec_cc=1,
-                            insert_threshold_p1=2.0, insert_threshold_p2=2.0)
+    return P.default_params(**{**WORKLOAD, "device_id": device_id, "Ny": Ny})
 
 
 def workload_synth(P, seed=1):
-    return P.synth_params(NX, NY, ppp=0.04, sigma=0.6, field=P.PIV_FIELD_VORTEX, a=10.0, b=600.0, c=0.002, seed=seed)
+    return P.synth_params(NX, NY, seed=seed, **SYNTH)
 
 
 def workload_pair(P, seed=1):
     return P.synth_pair(workload_synth(P, seed))
+
+
+def bench_config(nvec, world):
+    """The `config` of both arms' lines (identical keys and values)."""
+    return {"workload": "6600x4400 pair, MHE 40/0.91, grid 64x64@32 x2 -> 32x32@16 x3",
+            "vectors_per_pair": nvec, "pairs_per_step_per_gpu": 1, "parallelism": f"replicas x{world}",
+            "l2": "each step's working set (58 MB of frames, 117 MB deformed frame, GB-scale FFT buffers in the "
+                  "reference) exceeds the 126 MB L2; the device-resident line also flushes L2 (512 MB write) "
+                  "before every timed step"}
 
 
 def accuracy(P, e, s):
@@ -410,9 +432,7 @@ def run_ours(args, rank, world, local):
         "warmup": args.warmup, "ms_per_step": round(total_s * 1e3 / args.steps, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded particle images, Lamb-Oseen vortex + shear)",
-        "config": {"workload": "6600x4400 pair, MHE 40/0.91, grid 64x64@32 x2 -> 32x32@16 x3",
-                   "vectors_per_pair": nvec, "pairs_per_step_per_gpu": 1, "parallelism": f"replicas x{world}",
-                   "l2": "flushed (512 MB write) before every timed step", "xcorr_autotune": tuned},
+        "config": bench_config(nvec, world), "xcorr_autotune": tuned,
         "e2e": e2e, "roofline": roofline, "gpu_launches": launches, "clocks": clk.summary(),
         "accuracy": acc,
     }
@@ -434,17 +454,26 @@ def run_ours(args, rank, world, local):
 
 
 def run_reference(args, rank, world, local):
+    """The reference's own engine (oracle/_ref, compiled for sm_100a from its sources) on the
+    same pair, driven through xcorr2d_multi / mhe_gpu in X/main.cpp order.  This process
+    loads only the reference library, the CPU oracle (geometry) and the stand-alone
+    generator (oracle/libsynth.so): no part of the CUDA engine."""
     if rank != 0:
         return None
-    P = load_pkg()
+    import types
+
+    from oracle import oracle as O
     from oracle import ref as R
+    from oracle import synth as S
 
     if not R.available():
         return {"impl": "reference", "unavailable": "oracle/_ref/libref_xcorr2d.so was not built"}
-    p = workload_params(P, device_id=local)
-    f1, f2 = workload_pair(P, seed=1)
-    geom = P.geometry(p)
-    nvec = geom["Nt_vec"][1]
+    p = types.SimpleNamespace(**{**WORKLOAD, "device_id": local})
+    f1, f2 = S.pair(S.params(NX, NY, seed=1, **SYNTH))
+    rc, g = O.geometry(O.params_from(p))
+    if rc != 0:
+        return {"impl": "reference", "unavailable": f"geometry rejected ({rc})"}
+    nvec = g.Nt_vec[1]
     with R.RefEngine(p) as r:
         for _ in range(args.warmup):
             r.run_pair(f1, f2)
@@ -453,21 +482,25 @@ def run_reference(args, rank, world, local):
             t0 = time.perf_counter()
             for _ in range(args.steps):
                 r.run_pair(f1, f2)  # synchronises the device before returning
-                r.filtered(1, nvec)
+                dx, dy, vv = r.filtered(1, nvec)
             dt = time.perf_counter() - t0
     value = args.steps * nvec / dt
+    n = NX * NY
+    # per pair: MHE uploads both raw frames and reads both enhanced frames back
+    # (X/main.cpp:267-283); prep_img_data uploads each frame into both grids' buffers
+    # (X/xcorr2d_multi_grid.cu:1271-1282); the filtered grid-2 field is read back
+    h2d, d2h = 2 * n + 4 * n, 2 * n + int(dx.nbytes + dy.nbytes + vv.nbytes)
     return {
         "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(dt * 1e3 / args.steps, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "impl": "reference",
         "data": "synthetic (seeded particle images, Lamb-Oseen vortex + shear)",
-        "config": {"workload": "6600x4400 pair, MHE 40/0.91, grid 64x64@32 x2 -> 32x32@16 x3",
-                   "vectors_per_pair": nvec, "pairs_per_step_per_gpu": 1, "parallelism": "replicas x1"},
+        "config": bench_config(nvec, 1),
         "cpu_baseline": {"value": round(value, 1), "unit": UNIT, "cores": 1, "kind": "reference",
                          "sample": "the reference's CUDA engine compiled for sm_100a from its own sources, driven "
                                    "from one host thread through xcorr2d_multi/mhe_gpu in main.cpp order "
-                                   "(pinned host frames in, filtered grid-2 field out, wall clock)"},
-        "e2e": {"value": round(value, 1), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+                                   "(host frames in, filtered grid-2 field out, wall clock)"},
+        "e2e": {"value": round(value, 1), "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "clocks": clk.summary(),
     }
 

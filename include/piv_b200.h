@@ -316,16 +316,18 @@ int piv_mhe_process(piv_mhe *m, const uint8_t *d_in, uint8_t *d_out, void *strea
 int piv_mhe_destroy(piv_mhe *m);
 
 /* MHE of one frame without any allocation (no counterpart in the reference).  For callers
- * that cannot call cudaMalloc where they enhance a frame: code inside a CUDA graph capture,
- * real-time acquisition callbacks, applications whose own pool owns all device memory.
- * Same result as piv_mhe_process (d_in -> d_out, Nx*Ny device bytes each, outside the
- * centred crop written 0), but the tile histograms live in a fixed device array of the
- * library: PIV_MHE_NOALLOC_MAX_TILES tiles including the one-tile border ring, i.e.
- * (Ny/ws + 2) * (Nx/ws + 2) <= 24576 (24 MiB, held by every GPU that loads the library
- * until exit).  Larger requests return PIV_ERR_ARG with a message on stderr.  The first
- * call on a device looks up the array's device address; make that first call before any
- * stream capture.  All calls share the array: calls whose work overlaps on the GPU (other
- * streams, other threads) race and must be serialised by the caller. */
+ * that cannot call cudaMalloc where they enhance a frame: real-time acquisition callbacks
+ * that must not wait on the allocator, and applications whose own pool owns all device
+ * memory after start-up.  Same result as piv_mhe_process (d_in -> d_out, Nx*Ny device
+ * bytes each, outside the centred crop written 0), but the tile histograms live in a
+ * fixed device array of the library: PIV_MHE_NOALLOC_MAX_TILES tiles including the
+ * one-tile border ring, i.e. (Ny/ws + 2) * (Nx/ws + 2) <= 24576 (24 MiB, held by every GPU
+ * that loads the library until exit).  Larger requests return PIV_ERR_ARG with a message
+ * on stderr.  The first call on a device (and the first after that device's context was
+ * re-created, e.g. by cudaDeviceReset) looks up the array's device address; make that
+ * first call before any stream capture.  All calls share the array and each clears the
+ * part it uses: calls whose work overlaps on the GPU (other streams, other threads) race
+ * and must be serialised by the caller. */
 #define PIV_MHE_NOALLOC_MAX_TILES 24576
 int piv_mhe_process_noalloc(const uint8_t *d_in, uint8_t *d_out, int Nx, int Ny, int ws, float thresh,
                             void *stream);

@@ -67,6 +67,8 @@ def lib():
         h.ref_run_pair_recording.argtypes = [_P, _U8P, _U8P, _FP, _FP, _FP, _FP]
         h.ref_median_only.argtypes = [_P]
         h.ref_get_raw.argtypes = [_P, C.c_int, _FP, _FP, _U8P]
+        h.ref_set_raw.argtypes = [_P, C.c_int, _FP, _FP, _U8P]
+        h.ref_validate.argtypes = [_P, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, C.c_int, C.c_int]
         h.ref_get_filtered.argtypes = [_P, C.c_int, _FP, _FP, _U8P]
         h.ref_get_peaks.argtypes = [_P, C.c_int, _I32P, _I32P, _FP]
         h.ref_get_cc.argtypes = [_P, C.c_int, C.c_int, C.c_int, _FP]
@@ -140,6 +142,21 @@ class RefEngine:
         v = np.empty(n, np.uint8)
         lib().ref_get_raw(self.h, grid, _p(dx, C.c_float), _p(dy, C.c_float), _p(v, C.c_uint8))
         return dx.reshape(nt, -1), dy.reshape(nt, -1), v.reshape(nt, -1)
+
+    def set_raw(self, grid, dx, dy, valid):
+        """Raw candidates [Nt][Npeak_save] into the reference's arrays of a grid."""
+        dx = np.ascontiguousarray(dx, np.float32)
+        dy = np.ascontiguousarray(dy, np.float32)
+        valid = np.ascontiguousarray(valid, np.uint8)
+        rc = lib().ref_set_raw(self.h, grid, _p(dx, C.c_float), _p(dy, C.c_float), _p(valid, C.c_uint8))
+        if rc:
+            raise RuntimeError(f"reference set_raw failed ({rc})")
+
+    def validate(self, grid, Npass_median, minN, rthr, ithr, Npass_smooth, iffill=1):
+        """The reference's MedianFilter_Smoothing_p1/_p2 on the grid's current raw candidates."""
+        rc = lib().ref_validate(self.h, grid, Npass_median, minN, rthr, ithr, Npass_smooth, iffill)
+        if rc:
+            raise RuntimeError(f"reference validation failed ({rc})")
 
     def filtered(self, grid, nt):
         dx = np.empty(nt, np.float32)

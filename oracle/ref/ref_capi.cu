@@ -172,6 +172,29 @@ int ref_median_only(ref_engine *e)
     return cudaDeviceSynchronize() == cudaSuccess ? 0 : -4;
 }
 
+/* Host -> the reference's raw candidate arrays of a grid ([Nt*Npeak_save] each), so that
+ * its validation can be run on candidates from elsewhere (the engine's). */
+int ref_set_raw(ref_engine *e, int grid, const float *dx, const float *dy, const uint8_t *valid)
+{
+    xcorr2d_multi &x = e->x;
+    size_t n = (size_t)(grid ? x.Nt2_vec : x.Nt1_vec) * x.Npeak_save;
+    cudaMemcpy(grid ? x.d_disp_x_p2 : x.d_disp_x_p1, dx, n * sizeof(float), cudaMemcpyHostToDevice);
+    cudaMemcpy(grid ? x.d_disp_y_p2 : x.d_disp_y_p1, dy, n * sizeof(float), cudaMemcpyHostToDevice);
+    cudaMemcpy(grid ? (void *)x.d_valid_p2 : (void *)x.d_valid_p1, valid, n, cudaMemcpyHostToDevice);
+    return cudaDeviceSynchronize() == cudaSuccess ? 0 : -4;
+}
+
+/* MedianFilter_Smoothing_p1 / _p2 (X/xcorr2d_multi_grid.cu:1451, :1766) on the current raw
+ * candidates of a grid; grid 1 always fills (the reference's p1 form has no switch). */
+int ref_validate(ref_engine *e, int grid, int Npass_median, int minN, float rthr, float ithr, int Npass_smooth,
+                 int iffill)
+{
+    bool ok = grid ? e->x.MedianFilter_Smoothing_p2(Npass_median, minN, rthr, ithr, Npass_smooth, iffill)
+                   : e->x.MedianFilter_Smoothing_p1(Npass_median, minN, rthr, ithr, Npass_smooth);
+    if (!ok) return -4;
+    return cudaDeviceSynchronize() == cudaSuccess ? 0 : -4;
+}
+
 /* Device state -> host.  grid 0/1; raw candidates [Nt*Npeak_save] and the filtered field [Nt]. */
 int ref_get_raw(ref_engine *e, int grid, float *dx, float *dy, uint8_t *valid)
 {

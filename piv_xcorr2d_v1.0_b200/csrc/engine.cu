@@ -12,6 +12,7 @@
 // There are no correlation-plane buffers: the fused kernel keeps them on chip.
 #include <cuda_runtime.h>
 
+#include <cctype>
 #include <cerrno>
 #include <cmath>
 #include <cstdarg>
@@ -27,6 +28,18 @@
 namespace piv {
 
 static int imax(int a, int b) { return a > b ? a : b; }
+
+// PIV_AUTOTUNE, read the same way by the engine's and the batch's tuners: unset, or any
+// value other than 0 / off / false / no (any case), leaves tuning on.  Every tile variant
+// of a shape computes the same bits, so tuning changes speed only.
+static bool autotune_enabled()
+{
+    const char *env = getenv("PIV_AUTOTUNE");
+    if (!env) return true;
+    std::string v(env);
+    for (char &c : v) c = (char)tolower((unsigned char)c);
+    return !(v == "0" || v == "off" || v == "false" || v == "no");
+}
 
 static int vec_count(int N, int sp)
 {
@@ -178,6 +191,10 @@ struct piv_engine {
     unsigned learned_gen = 0;
     float *d_pred2 = nullptr, *d_judge = nullptr, *h_judge = nullptr;
     std::string err;
+    // fault injection, read from the environment at piv_create (off by default):
+    // PIV_TEST_FAIL_ALLOC=k fails the engine's k-th device allocation (counted from piv_create),
+    // PIV_TEST_FILL_CAP=n caps the hole fill at n iterations
+    int fail_alloc_at = 0, n_allocs = 0, fill_cap = 0;
     bool timing = false;
     cudaEvent_t ev[6] = {};
     float stage_ms[5] = {};
@@ -215,6 +232,10 @@ template <typename T>
 int dalloc(piv_engine *e, T **ptr, size_t n)
 {
     if (n == 0) n = 1;
+    if (e->fail_alloc_at > 0 && ++e->n_allocs == e->fail_alloc_at) {
+        *ptr = nullptr;
+        return set_err(e, PIV_ERR_ALLOC, "cudaMalloc ERROR! (%zu bytes: injected failure)", n * sizeof(T));
+    }
     cudaError_t c = cudaMalloc((void **)ptr, n * sizeof(T));
     if (c != cudaSuccess) {
         *ptr = nullptr;
@@ -472,6 +493,7 @@ int do_validate(piv_engine *e, int k, int Npass_median, int minN, float thr, int
     v.list = gs.list;
     v.list_n = e->d_list_n;
     v.status = e->d_status;
+    v.fill_cap = e->fill_cap;
     CK(launch_validate(v, e->stream));
     return PIV_OK;
 }
@@ -587,8 +609,7 @@ int tune_xcorr(piv_engine *e)
         }
         return PIV_OK;
     }
-    const char *env = getenv("PIV_AUTOTUNE");
-    if (env && atoi(env) == 0) return PIV_OK;
+    if (!autotune_enabled()) return PIV_OK;
     const piv_params &p = e->p;
     cudaStream_t s = e->stream;
     CK(launch_pattern(e->d_f1, nullptr, e->pitch, e->pitch, e->rows, 1u, s));
@@ -720,6 +741,8 @@ int piv_create(const piv_params *p, piv_engine **out)
     };
     if (cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess)
         return bail(set_err(e, PIV_ERR_CUDA, "stream creation failed"));
+    if (const char *v = getenv("PIV_TEST_FAIL_ALLOC")) e->fail_alloc_at = atoi(v);
+    if (const char *v = getenv("PIV_TEST_FILL_CAP")) e->fill_cap = atoi(v);
     // frame padding: every window of both grids reads inside the buffer
     int mx = 0, my = 0;
     const int wsx[2] = {p->ws_x1, p->ws_x2}, wsy[2] = {p->ws_y1, p->ws_y2};
@@ -1555,6 +1578,7 @@ struct piv_batch {
         float tuned_ms[2] = {};
     };
     std::vector<Group> groups;
+    std::vector<int> paths;  // each engine's (grid 1, grid 2) correlation path the groups were built for
     bool tuned = false;
     cudaGraphExec_t exec = nullptr;
     std::vector<const uint8_t *> graph_in;
@@ -1593,9 +1617,17 @@ void batch_free(piv_batch *b)
         if (e) piv_destroy(e);
 }
 
-// the groups' argument tables (the engines' buffers are fixed after creation)
+// the groups' argument tables (the engines' buffers are fixed after creation).  Only
+// pairs on the FP32 SIMT path join a group; a pair whose engine is set to a tensor-core
+// path runs its own tensor-core launch on its branch of the batch graph.
 int batch_build_groups(piv_batch *b)
 {
+    b->groups.clear();
+    b->paths.clear();
+    for (piv_engine *e : b->eng) {
+        b->paths.push_back(e->grid[0].path);
+        b->paths.push_back(e->grid[1].path);
+    }
     for (int k = 0; k < 2; ++k)
         for (int d = 0; d < 2; ++d) {
             for (int i = 0; i < b->n; ++i) {
@@ -1606,6 +1638,7 @@ int batch_build_groups(piv_batch *b)
                 if (!deformed && k == 1) continue;   // grid 2 passes are all deformed
                 if (deformed && k == 0 && np < 2) continue;
                 const GridState &gs = e->grid[k];
+                if (gs.path != PIV_XCORR_SIMT) continue;
                 const int K = gs.gg.Nps <= 4 ? 4 : 8;
                 piv_batch::Group *grp = nullptr;
                 for (auto &g : b->groups)
@@ -1636,7 +1669,7 @@ int batch_build_groups(piv_batch *b)
                 xb.first[0] = 0;
                 for (int j = 0; j < xb.n; ++j) {
                     xb.pairs[j] = xcorr_args(b->eng[g.pairs[c0 + j]], g.k);
-                    const int nw = xb.pairs[j].w_end - xb.pairs[j].w_first;
+                    const int nw = xb.pairs[j].w_end - (xb.pairs[j].w_first & ~1);
                     xb.first[j + 1] = xb.first[j] + (nw + B - 1) / B;
                 }
                 xb.items = xb.first[xb.n];
@@ -1705,9 +1738,12 @@ int batch_enqueue(piv_batch *b)
                 if (!deformed) {
                     CK(cudaMemsetAsync(gs.fx, 0, sizeof(float) * gs.gg.Nt_vec, e->stream));
                     CK(cudaMemsetAsync(gs.fy, 0, sizeof(float) * gs.gg.Nt_vec, e->stream));
-                    return PIV_OK;
+                } else {
+                    const int r = do_deform(e, k);
+                    if (r) return r;
                 }
-                return do_deform(e, k);
+                // a pair on a tensor-core path correlates on its own branch
+                return gs.path == PIV_XCORR_SIMT ? PIV_OK : do_xcorr(e, k, deformed, 0, 0, nullptr);
             });
             for (auto &g : b->groups)
                 if (!rc && g.k == k && g.deformed == deformed) rc = batch_launch_group(b, g, g.variant);
@@ -1729,8 +1765,14 @@ int batch_tune(piv_batch *b)
     int rc = batch_enqueue(b);
     if (rc) return rc;
     BCK(cudaStreamSynchronize(b->stream));
-    const char *env = getenv("PIV_AUTOTUNE");
-    if (env && env[0] == '0') return PIV_OK;
+    if (const char *fixed = getenv("PIV_BATCH_VARIANT")) {
+        // every group's variant by index (taken modulo the group's count), no timing
+        const int v = atoi(fixed);
+        if (v < 0) return batch_err(b, PIV_ERR_ARG, "PIV_BATCH_VARIANT wants a non-negative index");
+        for (auto &g : b->groups) g.variant = v % g.n_variants;
+        return PIV_OK;
+    }
+    if (!autotune_enabled()) return PIV_OK;
     cudaEvent_t t0, t1;
     BCK(cudaEventCreate(&t0));
     BCK(cudaEventCreate(&t1));
@@ -1836,6 +1878,18 @@ int piv_batch_run(piv_batch *b)
     for (piv_engine *e : b->eng)
         if (e->pending_slot >= 0) return batch_err(b, PIV_ERR_STATE, "a queued pair is pending on an engine");
     int rc;
+    std::vector<int> paths;
+    for (piv_engine *e : b->eng) {
+        paths.push_back(e->grid[0].path);
+        paths.push_back(e->grid[1].path);
+    }
+    if (paths != b->paths) {
+        // a member engine's correlation path changed: regroup, retune, recapture
+        if ((rc = batch_build_groups(b))) return rc;
+        b->tuned = false;
+        if (b->exec) cudaGraphExecDestroy(b->exec);
+        b->exec = nullptr;
+    }
     if (!b->tuned) {
         if ((rc = batch_tune(b))) return rc;
         b->tuned = true;

@@ -166,4 +166,38 @@ __device__ __forceinline__ void fft2t(float2 (&y)[N / 2], int half, unsigned mas
     });
 }
 
+// One-thread transform with exactly the arithmetic of fft2t: the even and odd halves by
+// fft<N/2>, then X[k] = E[k] + t, X[k + N/2] = E[k] - t with t = W^j O[k] for k = j < N/4
+// and t = (W^(N/4)) (W^j O[k]) for k = N/4 + j.  A CTA shape that runs a transform on one
+// thread therefore produces the same bits as one that runs it on a lane pair, so the
+// tile variant the autotuner picks never changes a result.
+template <int N, bool INV>
+__device__ __forceinline__ void fft_r2(float2 (&x)[N])
+{
+    static_assert(N % 4 == 0, "radix-2-first transform of a length divisible by 4");
+    constexpr int H = N / 2, Q = N / 4;
+    float2 e[H], o[H];
+#pragma unroll
+    for (int j = 0; j < H; ++j) {
+        e[j] = x[2 * j];
+        o[j] = x[2 * j + 1];
+    }
+    fft<H, INV>(e);
+    fft<H, INV>(o);
+    static_for<0, Q>([&](auto jc) {
+        constexpr int j = decltype(jc)::value;
+        const float2 t0 = twiddle<N, INV, j>(o[j]);
+        x[j] = cadd(e[j], t0);
+        x[j + H] = csub(e[j], t0);
+        const float2 t1 = rot_quarter<INV>(twiddle<N, INV, j>(o[j + Q]));
+        x[j + Q] = cadd(e[j + Q], t1);
+        x[j + Q + H] = csub(e[j + Q], t1);
+    });
+}
+
+// The inverse transform of the correlation kernels' P3/P4 phases: lengths of 32 and more
+// (divisible by 4) always split radix-2 first, whether one thread or a lane pair runs it.
+template <int N>
+constexpr bool inverse_radix2_first() { return N % 4 == 0 && N >= 32; }
+
 }  // namespace piv

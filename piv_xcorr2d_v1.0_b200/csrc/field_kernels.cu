@@ -461,13 +461,15 @@ __global__ void __launch_bounds__(128) median_pass_kernel(const MedianPass a)
 // invalid, 1 valid, 2 filled in this iteration (not yet a source, as in the
 // reference's two-kernel update).  The iteration count is capped at Nx+Ny+2 (the
 // fill front advances at least one cell per iteration while anything changes); the
-// cap sets a status bit instead of spinning.
+// cap sets a status bit instead of spinning.  cap_override > 0 lowers the cap (fault
+// injection: a wide hole then hits it).
 __global__ void __launch_bounds__(1024) fill_kernel(float *fx, float *fy, uint8_t *fv, int Nx, int Ny,
-                                                    const int *list, const int *list_n, int *status)
+                                                    const int *list, const int *list_n, int *status,
+                                                    int cap_override)
 {
     __shared__ int s_cnt[2];
     const int n = *list_n;
-    const int cap = Nx + Ny + 2;
+    const int cap = cap_override > 0 ? cap_override : Nx + Ny + 2;
     if (threadIdx.x < 2) s_cnt[threadIdx.x] = 0;
     __syncthreads();
     for (int it = 0; it < cap; ++it) {
@@ -589,7 +591,7 @@ cudaError_t launch_validate(const ValidateArgs &a, cudaStream_t s)
     }
     if (a.iffill) {
         fill_kernel<<<1, 1024, 0, s>>>(const_cast<float *>(cx), const_cast<float *>(cy), const_cast<uint8_t *>(cv),
-                                       a.Nx_vec, a.Ny_vec, a.list, a.list_n, a.status);
+                                       a.Nx_vec, a.Ny_vec, a.list, a.list_n, a.status, a.fill_cap);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
     for (int k = 0; k < a.Npass_smooth; ++k) {

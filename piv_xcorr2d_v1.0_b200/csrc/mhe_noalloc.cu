@@ -1,17 +1,22 @@
 // mhe_noalloc.cu -- MHE contrast enhancement that allocates nothing.
 //
 // Some callers cannot call cudaMalloc at the point where they want to enhance a frame:
-// code running while a CUDA graph is being captured (an allocation synchronises the
-// device and breaks the capture), real-time acquisition callbacks that must not wait
-// on the allocator, and host applications that hand all device memory to their own
-// pool and forbid plugins from allocating after start-up.  For them this entry point
-// runs the same two MHE kernels as piv_mhe_process, with the per-tile histogram grid
-// (the kernels' only scratch) in a fixed device array that the library owns.
+// real-time acquisition callbacks that must not wait on the allocator (an allocation can
+// synchronise the device), and host applications that hand all device memory to their
+// own pool at start-up and forbid plugins from allocating afterwards.  For them this
+// entry point runs the same two MHE kernels as piv_mhe_process, with the per-tile
+// histogram grid (the kernels' only scratch) in a fixed device array that the library
+// owns.
 //
 // The array is a file-scope __device__ variable: every GPU that loads this library
 // holds it (24 MiB) until the process exits.  In host code the symbol g_mhe_scratch
 // is a host-side stand-in, not a device address, so the host asks the runtime for the
-// device address once per device and passes that pointer to the kernels.
+// device address and passes that pointer to the kernels.  The address is looked up
+// once per device context: on the first call on a device, and again when that device's
+// context has been re-created (after cudaDeviceReset the module is loaded anew and the
+// array may sit elsewhere).  Contexts are told apart by their unique ID (cuCtxGetId),
+// not by their handle, which a new context may reuse.
+#include <cuda.h>
 #include <cstdio>
 #include <mutex>
 
@@ -25,21 +30,61 @@ static __device__ __align__(256) int g_mhe_scratch[kMaxLevels];
 
 constexpr int kMaxDevices = 64;
 std::mutex g_mu;
-int *g_dev_ptr[kMaxDevices] = {};
+struct Cached {
+    unsigned long long ctx = 0;  // unique ID of the context the address belongs to
+    int *ptr = nullptr;
+};
+Cached g_cache[kMaxDevices];
 
-// Device address of g_mhe_scratch on the current device (set up on first use).
+typedef CUresult (*CtxGetCurrentFn)(CUcontext *);
+typedef CUresult (*CtxGetIdFn)(CUcontext, unsigned long long *);
+CtxGetCurrentFn g_get_current = nullptr;
+CtxGetIdFn g_get_id = nullptr;
+bool g_resolved = false;
+
+// Unique ID of the calling thread's current context, 0 if there is none (or the driver
+// offers no context IDs).  Called with g_mu held.
+unsigned long long current_context_id()
+{
+    if (!g_resolved) {
+        g_resolved = true;
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            g_get_current = reinterpret_cast<CtxGetCurrentFn>(f);
+        f = nullptr;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetId", &f, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            g_get_id = reinterpret_cast<CtxGetIdFn>(f);
+    }
+    if (!g_get_current || !g_get_id) return 0;
+    CUcontext c = nullptr;
+    unsigned long long id = 0;
+    if (g_get_current(&c) != CUDA_SUCCESS || !c) return 0;
+    if (g_get_id(c, &id) != CUDA_SUCCESS) return 0;
+    return id;
+}
+
+// Device address of g_mhe_scratch in the current device's current context.
 int scratch_ptr(int **out)
 {
     int dev = -1;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return PIV_ERR_CUDA;
     std::lock_guard<std::mutex> lock(g_mu);
-    if (!g_dev_ptr[dev]) {
+    Cached &c = g_cache[dev];
+    const unsigned long long ctx = current_context_id();
+    if (!c.ptr || ctx == 0 || ctx != c.ctx) {
         void *p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&p, g_mhe_scratch);
-        if (e != cudaSuccess || !p) return PIV_ERR_CUDA;
-        g_dev_ptr[dev] = static_cast<int *>(p);
+        if (e != cudaSuccess || !p) {
+            c = Cached{};
+            return PIV_ERR_CUDA;
+        }
+        c.ptr = static_cast<int *>(p);
+        c.ctx = current_context_id();  // the lookup made the device's context current
     }
-    *out = g_dev_ptr[dev];
+    *out = c.ptr;
     return PIV_OK;
 }
 

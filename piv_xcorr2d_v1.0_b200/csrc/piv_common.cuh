@@ -195,6 +195,7 @@ struct ValidateArgs {
     int wx_sm, wy_sm, Npass_smooth, iffill;
     int *list, *list_n;  // fill work list [Nt_vec] and its length (device)
     int *status;         // device status word (bit 0: fill iteration cap)
+    int fill_cap;        // hole-fill iteration cap; <= 0: Nx_vec + Ny_vec + 2
 };
 cudaError_t launch_validate(const ValidateArgs &a, cudaStream_t s);
 

@@ -431,8 +431,8 @@ __global__ void __launch_bounds__(NT, (xcorr_min_ctas<WSX, WSY, B, NT>())) xcorr
 template <int WSX, int WSY, int B, int NT>
 cudaError_t launch_shape(const XcorrArgs &a, bool deformed, int K, cudaStream_t s)
 {
-    const int n = a.w_end - a.w_first;
-    if (n <= 0) return cudaSuccess;
+    if (a.w_end <= a.w_first) return cudaSuccess;
+    const int n = a.w_end - (a.w_first & ~1);  // CTAs start at an even window (pairing)
     const size_t smem = (size_t)B * WSY * (WSX + 1) * sizeof(float2);
     dim3 grid((n + B - 1) / B);
     cudaError_t e = cudaSuccess;

@@ -1,12 +1,13 @@
 """The allocation-free MHE entry point (piv_mhe_process_noalloc) against the allocating one.
 
-Callers that cannot allocate device memory where they enhance a frame (inside a graph
-capture, in real-time acquisition callbacks, under an application-owned memory pool) use
-piv_mhe_process_noalloc, which keeps its tile histograms in a fixed array of the library.
-This checks, through the C-ABI, that two calls in a row -- a full 6600x4400 frame, then a
-smaller frame with a different tile grid, so the second call starts from the first call's
-leftovers in the shared array -- give exactly the output of piv_mhe_process (MHE is
-integer arithmetic: bit-exact), and that requests larger than the array are refused.
+Callers that cannot allocate device memory where they enhance a frame (real-time
+acquisition callbacks that must not wait on the allocator, applications whose own pool owns
+all device memory) use piv_mhe_process_noalloc, which keeps its tile histograms in a fixed
+array of the library.  This checks, through the C-ABI, that calls in a row -- a full
+6600x4400 frame, then a smaller frame with a different tile grid, then a mid-size frame whose
+tile grid is larger than the previous call's, so each call starts from the previous call's
+leftovers in the shared array -- give exactly the output of piv_mhe_process (MHE is integer
+arithmetic: bit-exact), and that requests larger than the array are refused.
 Collected last (file name) so that a stop-at-first-failure run has already run the rest.
 """
 import ctypes as C
@@ -46,7 +47,7 @@ def no_alloc(d_in, Nx, Ny, ws, thresh):
 def test_no_alloc_mhe_matches_allocating_entry_point(cuda):
     import torch
 
-    cases = [(6600, 4400, 40, 0.91, 1), (333, 251, 16, 0.5, 2)]
+    cases = [(6600, 4400, 40, 0.91, 1), (333, 251, 16, 0.5, 2), (2048, 1536, 24, 0.8, 3)]
     for Nx, Ny, ws, th, seed in cases:
         f, _ = P.synth_pair(P.synth_params(Nx, Ny, ppp=0.04, seed=seed))
         d = torch.from_numpy(np.ascontiguousarray(f)).cuda()
