@@ -12,6 +12,7 @@
 // There are no correlation-plane buffers: the fused kernel keeps them on chip.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cctype>
 #include <cerrno>
 #include <cmath>
@@ -136,6 +137,11 @@ struct GridState {
     bool has_pass = false;
     int variant = 0;          // fused-kernel instantiation chosen by the autotuner
     int path = PIV_XCORR_SIMT;  // correlation path (PIV_XCORR_*)
+    // generic-size kernel (xcorr_generic.cu): shapes without a fused instance, or more
+    // than 8 saved peaks; planes above 20,480 points live in a workspace of gws_ctas slabs
+    bool generic = false;
+    float2 *gws = nullptr;
+    int gws_ctas = 0;
     float tuned_ms[8] = {};   // measured time per variant (0 = not measured)
     int n_tuned = 0;
 };
@@ -278,6 +284,7 @@ void free_all(piv_engine *e)
     cudaFree(e->d_status);
     cudaFree(e->d_list_n);
     for (auto &gs : e->grid) {
+        cudaFree(gs.gws);
         cudaFree(gs.cdx);
         cudaFree(gs.cdy);
         cudaFree(gs.cv);
@@ -375,6 +382,16 @@ XcorrArgs xcorr_args(piv_engine *e, int k)
     return a;
 }
 
+// The generic-size kernel's plane workspace of grid k, for planes too large for shared
+// memory (allocated at piv_create for the grids with passes, else at the first pass).
+int ensure_workspace(piv_engine *e, int k)
+{
+    GridState &gs = e->grid[k];
+    if (!gs.generic || gs.gws || !xcorr_generic_needs_workspace(gs.gg.ws_x, gs.gg.ws_y)) return PIV_OK;
+    gs.gws_ctas = imax(1, std::min(gs.gg.Nt_vec, xcorr_generic_ctas(gs.gg.ws_x, gs.gg.ws_y, gs.gg.Nps)));
+    return dalloc(e, &gs.gws, (size_t)gs.gws_ctas * gs.gg.ws_x * gs.gg.ws_y);
+}
+
 int do_xcorr(piv_engine *e, int k, bool deformed, int first, int end, float *dump)
 {
     GridState &gs = e->grid[k];
@@ -396,6 +413,7 @@ int do_xcorr(piv_engine *e, int k, bool deformed, int first, int end, float *dum
     a.status = e->d_status;
     const char *why = nullptr;
     auto launch = [&]() {
+        if (gs.generic) return launch_xcorr_generic(a, deformed, gs.gws, gs.gws_ctas, e->stream);
         if (gs.path == PIV_XCORR_SIMT) return launch_xcorr(a, deformed, e->stream, &why, gs.variant);
         return launch_xcorr_tc(a, deformed, e->stream, &why, gs.path == PIV_XCORR_TC_SPLIT ? 3 : 1);
     };
@@ -602,6 +620,7 @@ int tune_xcorr(piv_engine *e)
         if (sscanf(fixed, "%d,%d", &v[0], &v[1]) != 2) return set_err(e, PIV_ERR_ARG, "PIV_XCORR_VARIANT wants v1,v2");
         for (int k = 0; k < 2; ++k) {
             GridState &gs = e->grid[k];
+            if (gs.generic) continue;  // one form only
             if (v[k] < 0 || v[k] >= xcorr_variants(gs.gg.ws_x, gs.gg.ws_y))
                 return set_err(e, PIV_ERR_ARG, "PIV_XCORR_VARIANT: grid %d has %d variants", k + 1,
                                xcorr_variants(gs.gg.ws_x, gs.gg.ws_y));
@@ -620,7 +639,7 @@ int tune_xcorr(piv_engine *e)
     int rc = PIV_OK;
     for (int k = 0; k < 2 && !rc; ++k) {
         GridState &gs = e->grid[k];
-        if ((k == 0 ? p.Npass1 : p.Npass2) < 1) continue;
+        if ((k == 0 ? p.Npass1 : p.Npass2) < 1 || gs.generic) continue;
         const int nv = xcorr_variants(gs.gg.ws_x, gs.gg.ws_y);
         if (nv <= 1) continue;
         const bool deformed = gs.def != nullptr;
@@ -670,11 +689,9 @@ int validate_params(piv_engine *e, const piv_params &p)
     const char *why = nullptr;
     int rc = compute_geometry(p, e->g, &why);
     if (rc) return set_err(e, rc, "%s", why ? why : "invalid parameters");
-    if (!xcorr_supported(p.ws_x1, p.ws_y1) && p.Npass1 > 0)
-        return set_err(e, PIV_ERR_UNSUPPORTED, "grid-1 window %dx%d is not built into this engine", p.ws_x1, p.ws_y1);
-    if (!xcorr_supported(p.ws_x2, p.ws_y2) && p.Npass2 > 0)
-        return set_err(e, PIV_ERR_UNSUPPORTED, "grid-2 window %dx%d is not built into this engine", p.ws_x2, p.ws_y2);
-    if (p.Npeak_save > 8) return set_err(e, PIV_ERR_UNSUPPORTED, "Npeak_save > 8 is not built into this engine");
+    // every shape the geometry accepts runs: the fused kernels or the generic-size one
+    if (p.Npeak_save > kGenericMaxPeaks)
+        return set_err(e, PIV_ERR_ARG, "Npeak_save above %d is not supported", kGenericMaxPeaks);
     if (p.Npass1 < 0 || p.Npass2 < 0) return set_err(e, PIV_ERR_ARG, "negative pass count");
     if (p.if_mhe == 1 && !mhe_geometry(p.Nx, p.Ny, p.mhe_ws, p.mhe_thresh, e->mg))
         return set_err(e, PIV_ERR_ARG, "invalid MHE window/threshold");
@@ -827,6 +844,9 @@ int piv_create(const piv_params *p, piv_engine **out)
             if ((rc = dalloc(e, &gs.def, nd))) return bail(rc);
             cudaMemset(gs.def, 0, nd * sizeof(float));
         }
+        const char *force = getenv("PIV_XCORR_GENERIC");  // the generic kernel for every shape
+        gs.generic = !xcorr_supported(gg.ws_x, gg.ws_y) || Nps > 8 || (force && atoi(force) == 1);
+        if (((k == 0) ? p->Npass1 > 0 : p->Npass2 > 0) && (rc = ensure_workspace(e, k))) return bail(rc);
     }
     if ((rc = tune_xcorr(e))) return bail(rc);
     if (const char *path = getenv("PIV_XCORR_PATH")) {
@@ -834,7 +854,8 @@ int piv_create(const piv_params *p, piv_engine **out)
         // for every grid whose window shape the tensor-core path covers
         const int want = !strcmp(path, "tc") ? PIV_XCORR_TC_SPLIT : !strcmp(path, "tc1") ? PIV_XCORR_TC_BF16 : PIV_XCORR_SIMT;
         for (int k = 0; k < 2; ++k)
-            if (xcorr_tc_supported(e->grid[k].gg.ws_x, e->grid[k].gg.ws_y)) e->grid[k].path = want;
+            if (xcorr_tc_supported(e->grid[k].gg.ws_x, e->grid[k].gg.ws_y) && !e->grid[k].generic)
+                e->grid[k].path = want;
     }
     if (getenv("PIV_TIMING") && atoi(getenv("PIV_TIMING")) == 1) {
         e->timing = true;
@@ -956,8 +977,7 @@ int piv_pass_grid1(piv_engine *e, int idx_pass)
     int rc = check_ready(e, true);
     if (rc) return rc;
     if (idx_pass < 0) return set_err(e, PIV_ERR_ARG, "negative pass index");
-    if (!xcorr_supported(e->p.ws_x1, e->p.ws_y1))
-        return set_err(e, PIV_ERR_UNSUPPORTED, "grid-1 window shape not built");
+    if ((rc = ensure_workspace(e, 0))) return rc;
     if (idx_pass > 0 && !e->grid[0].def) {
         // the engine was created for a single grid-1 pass; deformation needs its buffer
         GridState &gs = e->grid[0];
@@ -987,8 +1007,7 @@ int piv_pass_grid2(piv_engine *e)
 {
     int rc = check_ready(e, true);
     if (rc) return rc;
-    if (!xcorr_supported(e->p.ws_x2, e->p.ws_y2))
-        return set_err(e, PIV_ERR_UNSUPPORTED, "grid-2 window shape not built");
+    if ((rc = ensure_workspace(e, 1))) return rc;
     if (!e->grid[1].def) {
         GridState &gs = e->grid[1];
         const size_t nd = (size_t)gs.def_pitch * gs.gg.Ny_aug;
@@ -1082,7 +1101,7 @@ int piv_run_pair_learned(piv_engine *e, piv_net *n, float max_reject_frac, float
     if (!n) return set_err(e, PIV_ERR_ARG, "null net");
     if (e->p.Npass2 < 1) return set_err(e, PIV_ERR_STATE, "the learned form needs grid-2 passes (Npass2 > 0)");
     if (e->p.ws_x1 < 8 || e->p.ws_y1 < 8) return set_err(e, PIV_ERR_UNSUPPORTED, "grid-1 windows under 8 px");
-    if (!xcorr_supported(e->p.ws_x2, e->p.ws_y2)) return set_err(e, PIV_ERR_UNSUPPORTED, "grid-2 window shape not built");
+    if ((rc = ensure_workspace(e, 1))) return rc;
     if (e->pending_slot >= 0) return set_err(e, PIV_ERR_STATE, "a queued pair is pending: use piv_run_pair");
     GridState &g1 = e->grid[0], &g2 = e->grid[1];
     if (!g2.def) {
@@ -1364,6 +1383,8 @@ int piv_set_xcorr_path(piv_engine *e, int grid, int path)
     GridState &gs = e->grid[grid];
     if (path != PIV_XCORR_SIMT && !xcorr_tc_supported(gs.gg.ws_x, gs.gg.ws_y))
         return set_err(e, PIV_ERR_UNSUPPORTED, "window shape %dx%d has no tensor-core path", gs.gg.ws_x, gs.gg.ws_y);
+    if (path != PIV_XCORR_SIMT && gs.generic)
+        return set_err(e, PIV_ERR_UNSUPPORTED, "the tensor-core path keeps at most 8 peaks per window");
     if (gs.path != path && (e->n_graphs || e->learned_exec)) {
         cudaStreamSynchronize(e->stream);
         for (int i = 0; i < e->n_graphs; ++i) cudaGraphExecDestroy(e->graphs[i].exec);
@@ -1386,6 +1407,12 @@ int piv_xcorr_config(const piv_engine *e, int grid, int *windows_per_cta, int *t
 {
     if (!e || grid < 0 || grid > 1) return PIV_ERR_ARG;
     const GridState &gs = e->grid[grid];
+    if (gs.generic) {
+        if (windows_per_cta) *windows_per_cta = 1;
+        if (threads_per_cta) *threads_per_cta = kGenericThreads;
+        if (tuned_ms) *tuned_ms = 0.f;
+        return PIV_OK;
+    }
     if (!xcorr_variant_shape(gs.gg.ws_x, gs.gg.ws_y, gs.variant, windows_per_cta, threads_per_cta))
         return PIV_ERR_UNSUPPORTED;
     if (tuned_ms) *tuned_ms = gs.n_tuned ? gs.tuned_ms[gs.variant] : 0.f;
@@ -1638,7 +1665,7 @@ int batch_build_groups(piv_batch *b)
                 if (!deformed && k == 1) continue;   // grid 2 passes are all deformed
                 if (deformed && k == 0 && np < 2) continue;
                 const GridState &gs = e->grid[k];
-                if (gs.path != PIV_XCORR_SIMT) continue;
+                if (gs.path != PIV_XCORR_SIMT || gs.generic) continue;
                 const int K = gs.gg.Nps <= 4 ? 4 : 8;
                 piv_batch::Group *grp = nullptr;
                 for (auto &g : b->groups)
@@ -1742,8 +1769,8 @@ int batch_enqueue(piv_batch *b)
                     const int r = do_deform(e, k);
                     if (r) return r;
                 }
-                // a pair on a tensor-core path correlates on its own branch
-                return gs.path == PIV_XCORR_SIMT ? PIV_OK : do_xcorr(e, k, deformed, 0, 0, nullptr);
+                // a pair on a tensor-core path or the generic-size kernel correlates on its own branch
+                return gs.path == PIV_XCORR_SIMT && !gs.generic ? PIV_OK : do_xcorr(e, k, deformed, 0, 0, nullptr);
             });
             for (auto &g : b->groups)
                 if (!rc && g.k == k && g.deformed == deformed) rc = batch_launch_group(b, g, g.variant);

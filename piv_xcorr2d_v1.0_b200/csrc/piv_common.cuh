@@ -199,6 +199,16 @@ struct ValidateArgs {
 };
 cudaError_t launch_validate(const ValidateArgs &a, cudaStream_t s);
 
+// Generic-size correlation kernel (xcorr_generic.cu): any ws_x, ws_y multiple of 4 in
+// [4, 1024] and up to kGenericMaxPeaks saved peaks.  Planes above 20,480 points need a
+// workspace of workspace_ctas * ws_x * ws_y complex values.
+constexpr int kGenericMaxPeaks = 1024;
+constexpr int kGenericThreads = 256;
+cudaError_t launch_xcorr_generic(const XcorrArgs &a, bool deformed, float2 *workspace, int workspace_ctas,
+                                 cudaStream_t s);
+bool xcorr_generic_needs_workspace(int wsx, int wsy);
+int xcorr_generic_ctas(int wsx, int wsy, int nps);
+
 // MHE (mhe_kernels.cu).
 struct MheGeom {
     int Nx, Ny, ws, width, height, xs, ys, maxI, maxJ, Ntrash, Nnontrash;
