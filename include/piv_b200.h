@@ -111,7 +111,14 @@ const char *piv_status_string(int status);
 
 /* mhe_gpu::init + xcorr2d_multi::init (X/MHE7_4_gpu.cu:149, X/xcorr2d_multi_grid.cu:716):
  * selects p->device_id, validates the geometry, allocates all device buffers and
- * the pinned host frame buffers, creates the engine stream. */
+ * the pinned host frame buffers, creates the engine stream.  Every window shape the
+ * reference accepts runs (ws_x, ws_y multiples of 4 in [4, 1024]): the fused register-FFT
+ * kernels cover 8..64 px in 13 shapes with up to 8 saved peaks, a generic-size kernel
+ * every other shape and Npeak_save up to 1024 (PIV_ERR_ARG above).  A pair's results do
+ * not depend on the tile variant, Nsec_cc, or whether it runs alone or in a batch.
+ * Fault injection (off unless set in the environment): PIV_TEST_FAIL_ALLOC=k fails the
+ * engine's k-th device allocation (PIV_ERR_ALLOC, everything freed); PIV_TEST_FILL_CAP=n
+ * caps the hole fill at n iterations (piv_synchronize then returns PIV_ERR_DEVICE). */
 int piv_create(const piv_params *p, piv_engine **out);
 
 /* xcorr2d_multi::freemem + mhe_gpu::freemem. */
@@ -268,14 +275,17 @@ int piv_get_stream(const piv_engine *e, void **stream);
 
 /* The fused correlation kernel configuration the autotuner chose for a grid at
  * piv_create (windows per CTA, threads per CTA) and its measured time per launch on
- * the tuning input (0 if not tuned; PIV_AUTOTUNE=0 keeps the defaults). */
+ * the tuning input (0 if not tuned; PIV_AUTOTUNE=0/off/false/no keeps the defaults,
+ * PIV_XCORR_VARIANT=v1,v2 fixes them).  The variants compute the same bits, so the
+ * choice changes speed only.  A grid on the generic-size kernel reports (1, 256, 0). */
 int piv_xcorr_config(const piv_engine *e, int grid, int *windows_per_cta, int *threads_per_cta, float *tuned_ms);
 
 /* Correlation path of a grid (0 = grid 1, 1 = grid 2).  PIV_XCORR_SIMT: register FFTs in FP32 on the CUDA cores
  * (default).  PIV_XCORR_TC_SPLIT: the transforms as DFT products on the tcgen05 tensor
  * cores with split-BF16 operands (hi*hi + hi*lo + lo*hi, FP32 accumulation).
  * PIV_XCORR_TC_BF16: one BF16 product per step (precision study only).  The tensor-core
- * paths cover square 16x16, 32x32 and 64x64 windows (PIV_ERR_UNSUPPORTED otherwise).
+ * paths cover square 16x16, 32x32 and 64x64 windows with up to 8 saved peaks
+ * (PIV_ERR_UNSUPPORTED otherwise).
  * PIV_XCORR_PATH=tc|tc1 in the environment at piv_create selects them for every grid
  * they cover. */
 #define PIV_XCORR_SIMT 0
@@ -370,8 +380,10 @@ int piv_synth_pair_device(const piv_synth_params *s, uint8_t *d_f1, uint8_t *d_f
  * captured graph: per pass, the pairs' deformations and validations on parallel
  * branches and ONE persistent correlation launch per (grid, window shape, top-K width)
  * group over all pairs in it, instead of one launch per pair.  The first run autotunes
- * each group's tile variant on the batch's data.  Results are bit-identical to
- * piv_run_pair on each engine.  Frames: set on each engine (piv_batch_engine +
+ * each group's tile variant on the batch's data (PIV_BATCH_VARIANT=v fixes it).  A pair
+ * whose engine is set to a tensor-core path (piv_set_xcorr_path), or whose shape runs on
+ * the generic-size kernel, correlates with its own launch on its branch of the graph.
+ * Results are bit-identical to piv_run_pair on each engine.  Frames: set on each engine (piv_batch_engine +
  * piv_set_images / piv_set_device_images / piv_host_images) before piv_batch_run; read
  * fields from the engines after piv_batch_synchronize.  Asynchronous. */
 typedef struct piv_batch piv_batch;
