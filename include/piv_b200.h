@@ -283,14 +283,18 @@ int piv_xcorr_config(const piv_engine *e, int grid, int *windows_per_cta, int *t
 /* Correlation path of a grid (0 = grid 1, 1 = grid 2).  PIV_XCORR_SIMT: register FFTs in FP32 on the CUDA cores
  * (default).  PIV_XCORR_TC_SPLIT: the transforms as DFT products on the tcgen05 tensor
  * cores with split-BF16 operands (hi*hi + hi*lo + lo*hi, FP32 accumulation).
- * PIV_XCORR_TC_BF16: one BF16 product per step (precision study only).  The tensor-core
- * paths cover square 16x16, 32x32 and 64x64 windows with up to 8 saved peaks
- * (PIV_ERR_UNSUPPORTED otherwise).
- * PIV_XCORR_PATH=tc|tc1 in the environment at piv_create selects them for every grid
- * they cover. */
+ * PIV_XCORR_TC_BF16: one BF16 product per step (precision study only).
+ * PIV_XCORR_TC_SPLIT_F16 / PIV_XCORR_TC_F16: the same with FP16 operands (about 22
+ * significant bits per split operand, 11 for one product; the passes' operands are scaled
+ * by exact powers of two that keep them in FP16's range).  The tensor-core paths cover
+ * square 16x16, 32x32 and 64x64 windows with up to 8 saved peaks (PIV_ERR_UNSUPPORTED
+ * otherwise).  PIV_XCORR_PATH=tc|tc1|tch|tch1 in the environment at piv_create selects
+ * them for every grid they cover. */
 #define PIV_XCORR_SIMT 0
 #define PIV_XCORR_TC_SPLIT 1
 #define PIV_XCORR_TC_BF16 2
+#define PIV_XCORR_TC_SPLIT_F16 3
+#define PIV_XCORR_TC_F16 4
 int piv_set_xcorr_path(piv_engine *e, int grid, int path);
 int piv_get_xcorr_path(const piv_engine *e, int grid, int *path);
 

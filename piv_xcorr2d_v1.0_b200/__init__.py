@@ -37,6 +37,8 @@ PIV_ERR_DEVICE = -8
 PIV_XCORR_SIMT = 0
 PIV_XCORR_TC_SPLIT = 1
 PIV_XCORR_TC_BF16 = 2
+PIV_XCORR_TC_SPLIT_F16 = 3
+PIV_XCORR_TC_F16 = 4
 
 PIV_FIELD_UNIFORM = 0
 PIV_FIELD_VORTEX = 1

@@ -415,7 +415,9 @@ int do_xcorr(piv_engine *e, int k, bool deformed, int first, int end, float *dum
     auto launch = [&]() {
         if (gs.generic) return launch_xcorr_generic(a, deformed, gs.gws, gs.gws_ctas, e->stream);
         if (gs.path == PIV_XCORR_SIMT) return launch_xcorr(a, deformed, e->stream, &why, gs.variant);
-        return launch_xcorr_tc(a, deformed, e->stream, &why, gs.path == PIV_XCORR_TC_SPLIT ? 3 : 1);
+        const bool split = gs.path == PIV_XCORR_TC_SPLIT || gs.path == PIV_XCORR_TC_SPLIT_F16;
+        const bool f16 = gs.path == PIV_XCORR_TC_SPLIT_F16 || gs.path == PIV_XCORR_TC_F16;
+        return launch_xcorr_tc(a, deformed, e->stream, &why, split ? 3 : 1, f16);
     };
     if (dump) {
         a.w_first = first;
@@ -852,7 +854,9 @@ int piv_create(const piv_params *p, piv_engine **out)
     if (const char *path = getenv("PIV_XCORR_PATH")) {
         // "tc": split-BF16 tensor-core path, "tc1": single-product BF16 (precision study),
         // for every grid whose window shape the tensor-core path covers
-        const int want = !strcmp(path, "tc") ? PIV_XCORR_TC_SPLIT : !strcmp(path, "tc1") ? PIV_XCORR_TC_BF16 : PIV_XCORR_SIMT;
+        const int want = !strcmp(path, "tc") ? PIV_XCORR_TC_SPLIT : !strcmp(path, "tc1") ? PIV_XCORR_TC_BF16
+                         : !strcmp(path, "tch") ? PIV_XCORR_TC_SPLIT_F16 : !strcmp(path, "tch1") ? PIV_XCORR_TC_F16
+                                                                                               : PIV_XCORR_SIMT;
         for (int k = 0; k < 2; ++k)
             if (xcorr_tc_supported(e->grid[k].gg.ws_x, e->grid[k].gg.ws_y) && !e->grid[k].generic)
                 e->grid[k].path = want;
@@ -1379,7 +1383,7 @@ int piv_debug_cc_planes(piv_engine *e, int grid, int first, int n, float *out)
 
 int piv_set_xcorr_path(piv_engine *e, int grid, int path)
 {
-    if (!e || grid < 0 || grid > 1 || path < PIV_XCORR_SIMT || path > PIV_XCORR_TC_BF16) return PIV_ERR_ARG;
+    if (!e || grid < 0 || grid > 1 || path < PIV_XCORR_SIMT || path > PIV_XCORR_TC_F16) return PIV_ERR_ARG;
     GridState &gs = e->grid[grid];
     if (path != PIV_XCORR_SIMT && !xcorr_tc_supported(gs.gg.ws_x, gs.gg.ws_y))
         return set_err(e, PIV_ERR_UNSUPPORTED, "window shape %dx%d has no tensor-core path", gs.gg.ws_x, gs.gg.ws_y);

@@ -155,7 +155,8 @@ int xcorr_variants(int ws_x, int ws_y);
 bool xcorr_variant_shape(int ws_x, int ws_y, int variant, int *windows_per_cta, int *threads_per_cta);
 // Tensor-core path (xcorr_tc.cuh): nprod 3 = split-BF16 (hi*hi + hi*lo + lo*hi), 1 = BF16.
 bool xcorr_tc_supported(int ws_x, int ws_y);
-cudaError_t launch_xcorr_tc(const XcorrArgs &a, bool deformed, cudaStream_t s, const char **why, int nprod);
+cudaError_t launch_xcorr_tc(const XcorrArgs &a, bool deformed, cudaStream_t s, const char **why, int nprod,
+                            bool f16);
 
 // Field kernels (field_kernels.cu).
 struct DeformArgs {

@@ -15,6 +15,7 @@
 // its transpose, without a second copy.
 #pragma once
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 
 #include <cstdint>
 
@@ -193,6 +194,25 @@ __device__ __forceinline__ void split_bf16x2(float a, float b, uint32_t &hi, uin
     const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
     const float2 hf = __bfloat1622float2(h);
     const __nv_bfloat162 l = __floats2bfloat162_rn(a - hf.x, b - hf.y);
+    hi = *reinterpret_cast<const uint32_t *>(&h);
+    lo = *reinterpret_cast<const uint32_t *>(&l);
+}
+
+// FP16 forms of the two splits (hi + lo carry about 22 significant bits; the caller keeps
+// the values inside FP16's range).
+__device__ __forceinline__ void split_f16(float x, uint16_t &hi, uint16_t &lo)
+{
+    const __half h = __float2half_rn(x);
+    const __half l = __float2half_rn(x - __half2float(h));
+    hi = __half_as_ushort(h);
+    lo = __half_as_ushort(l);
+}
+
+__device__ __forceinline__ void split_f16x2(float a, float b, uint32_t &hi, uint32_t &lo)
+{
+    const __half2 h = __floats2half2_rn(a, b);
+    const float2 hf = __half22float2(h);
+    const __half2 l = __floats2half2_rn(a - hf.x, b - hf.y);
     hi = *reinterpret_cast<const uint32_t *>(&h);
     lo = *reinterpret_cast<const uint32_t *>(&l);
 }

@@ -2,6 +2,8 @@
 // Every shape (WSX, WSY) is compiled in its own translation unit (xcorr_shape_*.cu) in
 // several variants (B windows per CTA, NT threads per CTA); the first listed variant of a
 // shape is its default, the engine's autotuner may pick another one per grid.
+#include <type_traits>
+
 #include "piv_common.cuh"
 
 namespace piv {
@@ -205,18 +207,21 @@ cudaError_t launch_xcorr(const XcorrArgs &a, bool deformed, cudaStream_t s, cons
 
 namespace piv {
 
-template <int WS, int NPROD>
+template <int WS, int NPROD, bool F16>
 cudaError_t launch_tc_shape(const XcorrArgs &a, bool deformed, int K, cudaStream_t s);
-extern template cudaError_t launch_tc_shape<16, 3>(const XcorrArgs &, bool, int, cudaStream_t);
-extern template cudaError_t launch_tc_shape<16, 1>(const XcorrArgs &, bool, int, cudaStream_t);
-extern template cudaError_t launch_tc_shape<32, 3>(const XcorrArgs &, bool, int, cudaStream_t);
-extern template cudaError_t launch_tc_shape<32, 1>(const XcorrArgs &, bool, int, cudaStream_t);
-extern template cudaError_t launch_tc_shape<64, 3>(const XcorrArgs &, bool, int, cudaStream_t);
-extern template cudaError_t launch_tc_shape<64, 1>(const XcorrArgs &, bool, int, cudaStream_t);
+#define PIV_TC(WS) \
+    extern template cudaError_t launch_tc_shape<WS, 3, false>(const XcorrArgs &, bool, int, cudaStream_t); \
+    extern template cudaError_t launch_tc_shape<WS, 1, false>(const XcorrArgs &, bool, int, cudaStream_t); \
+    extern template cudaError_t launch_tc_shape<WS, 3, true>(const XcorrArgs &, bool, int, cudaStream_t); \
+    extern template cudaError_t launch_tc_shape<WS, 1, true>(const XcorrArgs &, bool, int, cudaStream_t);
+PIV_TC(16)
+PIV_TC(32)
+PIV_TC(64)
+#undef PIV_TC
 
 bool xcorr_tc_supported(int wsx, int wsy) { return wsx == wsy && (wsx == 16 || wsx == 32 || wsx == 64); }
 
-cudaError_t launch_xcorr_tc(const XcorrArgs &a, bool deformed, cudaStream_t s, const char **why, int nprod)
+cudaError_t launch_xcorr_tc(const XcorrArgs &a, bool deformed, cudaStream_t s, const char **why, int nprod, bool f16)
 {
     if (a.g.Nps > 8) {
         if (why) *why = "Npeak_save > 8 is not built into this engine";
@@ -227,9 +232,14 @@ cudaError_t launch_xcorr_tc(const XcorrArgs &a, bool deformed, cudaStream_t s, c
         return cudaErrorInvalidValue;
     }
     const int K = a.g.Nps <= 4 ? 4 : 8;
-    if (a.g.ws_x == 16) return nprod == 3 ? launch_tc_shape<16, 3>(a, deformed, K, s) : launch_tc_shape<16, 1>(a, deformed, K, s);
-    if (a.g.ws_x == 32) return nprod == 3 ? launch_tc_shape<32, 3>(a, deformed, K, s) : launch_tc_shape<32, 1>(a, deformed, K, s);
-    return nprod == 3 ? launch_tc_shape<64, 3>(a, deformed, K, s) : launch_tc_shape<64, 1>(a, deformed, K, s);
+    auto pick = [&](auto ws) -> cudaError_t {
+        constexpr int WS = decltype(ws)::value;
+        if (f16) return nprod == 3 ? launch_tc_shape<WS, 3, true>(a, deformed, K, s) : launch_tc_shape<WS, 1, true>(a, deformed, K, s);
+        return nprod == 3 ? launch_tc_shape<WS, 3, false>(a, deformed, K, s) : launch_tc_shape<WS, 1, false>(a, deformed, K, s);
+    };
+    if (a.g.ws_x == 16) return pick(std::integral_constant<int, 16>{});
+    if (a.g.ws_x == 32) return pick(std::integral_constant<int, 32>{});
+    return pick(std::integral_constant<int, 64>{});
 }
 
 }  // namespace piv

@@ -21,10 +21,15 @@
 //   C  rows (window, kx)   x [re | im] over ky    * G^T  -> inverse column transforms
 //   D  rows (window, y)    x [re | im] over kx    * G^T[:, :WS] -> real correlation row
 // G lives once per CTA in shared memory; its K-major view is G^T, its MN-major view G
-// (layouts in tc_common.cuh).  Operands are BF16; NPROD = 3 splits every value into
-// hi + lo and accumulates hi*hi + hi*lo + lo*hi in FP32 (about 16 significant bits per
-// operand), NPROD = 1 uses the rounded values only (precision study).  |corr|/N goes to
-// fftshifted FP32 planes in shared memory and the peak stage is the SIMT kernel's.
+// (layouts in tc_common.cuh).  Operands are BF16 (F16 = false) or FP16 (F16 = true);
+// NPROD = 3 splits every value into hi + lo and accumulates hi*hi + hi*lo + lo*hi in FP32
+// (about 16 significant bits per operand in BF16, 22 in FP16), NPROD = 1 uses the rounded
+// values only (precision study).  FP16 has a 5-bit exponent, so the operands of passes B,
+// C and D are scaled by exact powers of two that keep every value of any 8-bit window pair
+// below 65504: pass B's by 1/WS, the cross spectrum by 1/(2 WS^2), pass D's by 1/(2 WS);
+// one multiply by a power of two at the end undoes them (the same scaling runs on the
+// BF16 path, whose rounding it leaves unchanged).  |corr|/N goes to fftshifted FP32
+// planes in shared memory and the peak stage is the SIMT kernel's.
 //
 // Waits on the MMA completion barrier are bounded: on a timeout the warpgroup stops,
 // sets bit kStatusMmaWait in *a.status, and the CTA releases its tensor memory.
@@ -52,32 +57,50 @@ constexpr TwTable<WS> make_tw()
 template <int WS>
 __constant__ TwTable<WS> kTw = make_tw<WS>();
 
-// 8 floats -> bf16 hi (and lo) as 16 bytes each
-__device__ __forceinline__ void split8(const float *v, uint4 &hi, uint4 &lo)
+// 8 floats -> bf16 / fp16 hi (and lo) as 16 bytes each
+template <bool F16>
+__device__ __forceinline__ void split2(float a, float b, uint32_t &hi, uint32_t &lo)
 {
-    tc::split_bf16x2(v[0], v[1], hi.x, lo.x);
-    tc::split_bf16x2(v[2], v[3], hi.y, lo.y);
-    tc::split_bf16x2(v[4], v[5], hi.z, lo.z);
-    tc::split_bf16x2(v[6], v[7], hi.w, lo.w);
+    if constexpr (F16) tc::split_f16x2(a, b, hi, lo);
+    else tc::split_bf16x2(a, b, hi, lo);
 }
 
-template <int NPROD>
+template <bool F16>
+__device__ __forceinline__ void split8(const float *v, uint4 &hi, uint4 &lo)
+{
+    split2<F16>(v[0], v[1], hi.x, lo.x);
+    split2<F16>(v[2], v[3], hi.y, lo.y);
+    split2<F16>(v[4], v[5], hi.z, lo.z);
+    split2<F16>(v[6], v[7], hi.w, lo.w);
+}
+
+template <int NPROD, bool F16>
 __device__ __forceinline__ void store8(uint8_t *hi, uint8_t *lo, uint32_t off, const float *v)
 {
     uint4 h, l;
-    split8(v, h, l);
+    split8<F16>(v, h, l);
     *reinterpret_cast<uint4 *>(hi + off) = h;
     if constexpr (NPROD > 1) *reinterpret_cast<uint4 *>(lo + off) = l;
+}
+
+// the 8 values scaled by a power of two, then stored as above
+template <int NPROD, bool F16>
+__device__ __forceinline__ void store8s(uint8_t *hi, uint8_t *lo, uint32_t off, const float *v, float scale)
+{
+    float w[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) w[i] = v[i] * scale;
+    store8<NPROD, F16>(hi, lo, off, w);
 }
 
 // One pass: D[128 x N] = A[128 x KK] * B^T over KK/16 K steps.  A in the K-major
 // (A_MN = false) or MN-major layout; B is the G buffer read MN-major (G) or K-major
 // (G^T).  The lo*hi product runs from K step LO_FROM on (A's lo part is zero before).
-template <int KK, int N, bool A_MN, bool B_MN, int NPROD, int LO_FROM>
+template <int KK, int N, bool A_MN, bool B_MN, int NPROD, int LO_FROM, bool F16>
 __device__ __forceinline__ void issue_pass(uint32_t tmem, uint32_t a_hi, uint32_t a_lo, uint32_t g_hi,
                                            uint32_t g_lo)
 {
-    constexpr uint32_t idesc = tc::idesc_f16(N, A_MN, B_MN, true);
+    constexpr uint32_t idesc = tc::idesc_f16(N, A_MN, B_MN, !F16);
     constexpr uint32_t a_lbo = A_MN ? 128u : 128u * 16u, a_sbo = A_MN ? KK * 16u : 128u;
     constexpr uint32_t a_step = A_MN ? 256u : 2u * a_lbo;
     constexpr uint32_t b_lbo = B_MN ? 128u : KK * 16u, b_sbo = B_MN ? KK * 16u : 128u;
@@ -146,7 +169,7 @@ struct TcShape {
     static constexpr size_t SMEM = 2 * (size_t)G_BYTES + (size_t)NG * 2 * A_BYTES;
 };
 
-template <int WS, int NPROD, int K, bool DEF>
+template <int WS, int NPROD, int K, bool DEF, bool F16>
 __global__ void __launch_bounds__(TcShape<WS>::THREADS, 1) xcorr_tc_kernel(const XcorrArgs a)
 {
     using S = TcShape<WS>;
@@ -155,7 +178,10 @@ __global__ void __launch_bounds__(TcShape<WS>::THREADS, 1) xcorr_tc_kernel(const
     constexpr int LDF = WS + 1;     // plane row stride (peak stage)
     constexpr uint32_t G_BYTES = S::G_BYTES, A_BYTES = S::A_BYTES;
     constexpr uint32_t TCOLS = S::TCOLS, TALLOC = S::TCOLS * S::NG;
-    constexpr float inv_n = 1.0f / (float)(WS * WS);
+    // operand scales (powers of two): pass B 1/WS, cross spectrum 1/(2 WS^2), pass D 1/(2 WS);
+    // the plane is |out| * (2 WS * 2 WS^2 * WS^2) / N = |out| * 4 WS^3, one exact multiply
+    constexpr float sB = 1.0f / (float)WS, sC = 1.0f / (float)(2 * WS * WS), sD = 1.0f / (float)(2 * WS);
+    constexpr float out_scale = (float)(4 * WS * WS * WS);
     static_assert(TALLOC == 32 || TALLOC == 64 || TALLOC == 128 || TALLOC == 256 || TALLOC == 512, "TMEM alloc");
     static_assert((size_t)NWIN * WS * LDF * 4 <= 2 * A_BYTES, "planes fit in the A buffers");
 
@@ -180,7 +206,8 @@ __global__ void __launch_bounds__(TcShape<WS>::THREADS, 1) xcorr_tc_kernel(const
         const float cv = kTw<WS>.c[q], sv = kTw<WS>.s[q];
         const float v = ((gr < WS) == (gc < WS)) ? cv : ((gr < WS) ? -sv : sv);
         uint16_t h, l;
-        tc::split_bf16(v, h, l);
+        if constexpr (F16) tc::split_f16(v, h, l);
+        else tc::split_bf16(v, h, l);
         const uint32_t o = (gc / 8) * (KK * 16) + gr * 16 + (gc % 8) * 2;
         *reinterpret_cast<uint16_t *>(g_hi + o) = h;
         *reinterpret_cast<uint16_t *>(g_lo + o) = l;
@@ -245,14 +272,14 @@ __global__ void __launch_bounds__(TcShape<WS>::THREADS, 1) xcorr_tc_kernel(const
             }
 #pragma unroll
             for (int c = 0; c < WS / 8; ++c) {
-                store8<NPROD>(a_hi, a_lo, tc::off_kmajor(lt, 8 * c, 128), v1 + 8 * c);
-                store8<NPROD>(a_hi, a_lo, tc::off_kmajor(lt, WS + 8 * c, 128), v2 + 8 * c);
+                store8<NPROD, F16>(a_hi, a_lo, tc::off_kmajor(lt, 8 * c, 128), v1 + 8 * c);
+                store8<NPROD, F16>(a_hi, a_lo, tc::off_kmajor(lt, WS + 8 * c, 128), v2 + 8 * c);
             }
         }
         if (!sync_issue(true)) break;
         if (lt == 0) {
             // frame 1 is integer-valued (exact in bf16); frame 2 only when deformed
-            issue_pass<KK, KK, false, true, NPROD, DEF ? WS / 16 : KK / 16>(tmem, sa_hi, sa_lo, sg_hi, sg_lo);
+            issue_pass<KK, KK, false, true, NPROD, DEF ? WS / 16 : KK / 16, F16>(tmem, sa_hi, sa_lo, sg_hi, sg_lo);
             tc::mma_commit(mb);
         }
 
@@ -272,8 +299,8 @@ __global__ void __launch_bounds__(TcShape<WS>::THREADS, 1) xcorr_tc_kernel(const
                         br[i] = zr[col_at<WS>(8 * c + i)];
                         bi[i] = zi[col_at<WS>(8 * c + i)];
                     }
-                    store8<NPROD>(a_hi, a_lo, tc::off_mnmajor(wl * WS + 8 * c, r, KK), br);
-                    store8<NPROD>(a_hi, a_lo, tc::off_mnmajor(wl * WS + 8 * c, WS + r, KK), bi);
+                    store8s<NPROD, F16>(a_hi, a_lo, tc::off_mnmajor(wl * WS + 8 * c, r, KK), br, sB);
+                    store8s<NPROD, F16>(a_hi, a_lo, tc::off_mnmajor(wl * WS + 8 * c, WS + r, KK), bi, sB);
                 }
             }
             if (!sync_issue(ok)) {
@@ -282,7 +309,7 @@ __global__ void __launch_bounds__(TcShape<WS>::THREADS, 1) xcorr_tc_kernel(const
             }
         }
         if (lt == 0) {
-            issue_pass<KK, KK, true, true, NPROD, 0>(tmem, sa_hi, sa_lo, sg_hi, sg_lo);
+            issue_pass<KK, KK, true, true, NPROD, 0, F16>(tmem, sa_hi, sa_lo, sg_hi, sg_lo);
             tc::mma_commit(mb);
         }
 
@@ -305,8 +332,8 @@ __global__ void __launch_bounds__(TcShape<WS>::THREADS, 1) xcorr_tc_kernel(const
                         cr[i] = 0.5f * (zr[ky] * pi + zi[ky] * pr);
                         ci[i] = 0.25f * ((pr * pr + pi * pi) - (zr[ky] * zr[ky] + zi[ky] * zi[ky]));
                     }
-                    store8<NPROD>(a_hi, a_lo, tc::off_kmajor(lt, 8 * c, 128), cr);
-                    store8<NPROD>(a_hi, a_lo, tc::off_kmajor(lt, WS + 8 * c, 128), ci);
+                    store8s<NPROD, F16>(a_hi, a_lo, tc::off_kmajor(lt, 8 * c, 128), cr, sC);
+                    store8s<NPROD, F16>(a_hi, a_lo, tc::off_kmajor(lt, WS + 8 * c, 128), ci, sC);
                 }
             }
             if (!sync_issue(ok)) {
@@ -315,7 +342,7 @@ __global__ void __launch_bounds__(TcShape<WS>::THREADS, 1) xcorr_tc_kernel(const
             }
         }
         if (lt == 0) {
-            issue_pass<KK, KK, false, false, NPROD, 0>(tmem, sa_hi, sa_lo, sg_hi, sg_lo);
+            issue_pass<KK, KK, false, false, NPROD, 0, F16>(tmem, sa_hi, sa_lo, sg_hi, sg_lo);
             tc::mma_commit(mb);
         }
 
@@ -329,8 +356,8 @@ __global__ void __launch_bounds__(TcShape<WS>::THREADS, 1) xcorr_tc_kernel(const
                 tc::tmem_wait_ld();
 #pragma unroll
                 for (int c = 0; c < WS / 8; ++c) {
-                    store8<NPROD>(a_hi, a_lo, tc::off_mnmajor(wl * WS + 8 * c, kx, KK), tr + 8 * c);
-                    store8<NPROD>(a_hi, a_lo, tc::off_mnmajor(wl * WS + 8 * c, WS + kx, KK), ti + 8 * c);
+                    store8s<NPROD, F16>(a_hi, a_lo, tc::off_mnmajor(wl * WS + 8 * c, kx, KK), tr + 8 * c, sD);
+                    store8s<NPROD, F16>(a_hi, a_lo, tc::off_mnmajor(wl * WS + 8 * c, WS + kx, KK), ti + 8 * c, sD);
                 }
             }
             if (!sync_issue(ok)) {
@@ -339,7 +366,7 @@ __global__ void __launch_bounds__(TcShape<WS>::THREADS, 1) xcorr_tc_kernel(const
             }
         }
         if (lt == 0) {
-            issue_pass<KK, WS, true, false, NPROD, 0>(tmem, sa_hi, sa_lo, sg_hi, sg_lo);
+            issue_pass<KK, WS, true, false, NPROD, 0, F16>(tmem, sa_hi, sa_lo, sg_hi, sg_lo);
             tc::mma_commit(mb);
         }
 
@@ -352,7 +379,7 @@ __global__ void __launch_bounds__(TcShape<WS>::THREADS, 1) xcorr_tc_kernel(const
                 tc::tmem_wait_ld();
                 float *prow = planes + wl * (WS * LDF) + ((r + WS / 2) % WS) * LDF;
 #pragma unroll
-                for (int x = 0; x < WS; ++x) prow[(x + WS / 2) % WS] = fabsf(cv[x]) * inv_n;
+                for (int x = 0; x < WS; ++x) prow[(x + WS / 2) % WS] = fabsf(cv[x]) * out_scale;
             }
             tc::fence_before_sync();
             const bool bad = tc::named_sync_or(bar_id, 128, !ok);
@@ -396,7 +423,7 @@ __global__ void __launch_bounds__(TcShape<WS>::THREADS, 1) xcorr_tc_kernel(const
 
 // Launch of one tensor-core shape: one CTA per SM (a kernel using tensor memory is
 // resident once per SM), persistent over the tiles.
-template <int WS, int NPROD>
+template <int WS, int NPROD, bool F16>
 cudaError_t launch_tc_shape(const XcorrArgs &a, bool deformed, int K, cudaStream_t s)
 {
     using S = TcShape<WS>;
@@ -416,11 +443,11 @@ cudaError_t launch_tc_shape(const XcorrArgs &a, bool deformed, int K, cudaStream
         e = cudaGetLastError();
     };
     if (K <= 4) {
-        if (deformed) go(xcorr_tc_kernel<WS, NPROD, 4, true>);
-        else go(xcorr_tc_kernel<WS, NPROD, 4, false>);
+        if (deformed) go(xcorr_tc_kernel<WS, NPROD, 4, true, F16>);
+        else go(xcorr_tc_kernel<WS, NPROD, 4, false, F16>);
     } else {
-        if (deformed) go(xcorr_tc_kernel<WS, NPROD, 8, true>);
-        else go(xcorr_tc_kernel<WS, NPROD, 8, false>);
+        if (deformed) go(xcorr_tc_kernel<WS, NPROD, 8, true, F16>);
+        else go(xcorr_tc_kernel<WS, NPROD, 8, false, F16>);
     }
     return e;
 }

@@ -1,7 +1,9 @@
-// Tensor-core correlation kernel, 64 x 64 windows (both precisions).
+// Tensor-core correlation kernel, 64 x 64 windows (split and single products, BF16 and FP16 operands).
 #include "xcorr_tc.cuh"
 
 namespace piv {
-template cudaError_t launch_tc_shape<64, 3>(const XcorrArgs &, bool, int, cudaStream_t);
-template cudaError_t launch_tc_shape<64, 1>(const XcorrArgs &, bool, int, cudaStream_t);
+template cudaError_t launch_tc_shape<64, 3, false>(const XcorrArgs &, bool, int, cudaStream_t);
+template cudaError_t launch_tc_shape<64, 3, true>(const XcorrArgs &, bool, int, cudaStream_t);
+template cudaError_t launch_tc_shape<64, 1, false>(const XcorrArgs &, bool, int, cudaStream_t);
+template cudaError_t launch_tc_shape<64, 1, true>(const XcorrArgs &, bool, int, cudaStream_t);
 }  // namespace piv

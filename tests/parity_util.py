@@ -33,7 +33,8 @@ def near_ties(planes, bx, by, nps, rel=1e-5):
     vals = np.where(cand, c, -np.inf).reshape(n, -1)
     top = -np.sort(-vals, axis=1)[:, :nps + 1]
     both = np.isfinite(top[:, 1:]) & np.isfinite(top[:, :-1])
-    tie_top = (both & (np.abs(np.diff(top, axis=1)) <= rel * top[:, :1])).any(1)
+    with np.errstate(invalid="ignore"):  # -inf - -inf where a window has few maxima
+        tie_top = (both & (np.abs(np.diff(top, axis=1)) <= rel * top[:, :1])).any(1)
     # the Npeak_save-th maximum (or 0 when there are fewer): a near-tie point above it ranks
     kth = top[:, min(nps, top.shape[1]) - 1]
     floor = np.where(np.isfinite(kth), kth - tol[:, 0, 0], 0.0)[:, None, None]
