@@ -318,14 +318,20 @@ __global__ void __launch_bounds__(kGenThreads) xcorr_generic_kernel(const XcorrA
         // ---- forward 2D transform: rows (x), then columns (y) ----
         gfft_dim<ANY>(plane, pl.fx, pl.nfx, nx, 1, ny, nx, Wx, false, false);
         gfft_dim<ANY>(plane, pl.fy, pl.nfy, ny, nx, nx, 1, Wy, false, true);
-        // ---- cross spectrum, in place over (k, -k) pairs ----
+        // ---- cross spectrum, in place over (k, -k) pairs.  Z(0,0) = (sum f1, sum f2) is
+        //      exactly zero iff a frame's window is all zero; the reference's correlation is
+        //      then exactly 0 (no candidate), so the spectrum is set to 0 ----
+        const float2 dc = plane[0];
+        const bool dead = dc.x == 0.f || dc.y == 0.f;
+        __syncthreads();  // every thread has read the DC term before it is overwritten
         for (int t = tid; t < N; t += blockDim.x) {
             const int ky = t / nx, kx = t - ky * nx;
             const int tm = ((ny - ky) % ny) * nx + (nx - kx) % nx;
             if (tm < t) continue;
             const float2 A = plane[t], M = plane[tm];
-            const float2 C = make_float2(0.5f * (A.x * M.y + A.y * M.x),
-                                         0.25f * ((M.x * M.x + M.y * M.y) - (A.x * A.x + A.y * A.y)));
+            const float2 C = dead ? make_float2(0.f, 0.f)
+                                  : make_float2(0.5f * (A.x * M.y + A.y * M.x),
+                                                0.25f * ((M.x * M.x + M.y * M.y) - (A.x * A.x + A.y * A.y)));
             plane[t] = C;
             if (tm != t) plane[tm] = make_float2(C.x, -C.y);
         }

@@ -158,6 +158,28 @@ __host__ __device__ constexpr int pos_of(int kx)
     }
 }
 
+// Whether window wl of a tile has an all-zero frame 1 or frame 2, from the pass-A row
+// ballots of the warpgroup's 4 warps (window wl owns rows [wl*WS, wl*WS + WS)).
+template <int WS>
+__device__ __forceinline__ bool window_dead(const uint32_t (&nz1)[4], const uint32_t (&nz2)[4], int wl)
+{
+    uint32_t a = 0, b = 0;
+    if constexpr (WS <= 32) {
+        const int warp = (wl * WS) >> 5, sh = (wl * WS) & 31;
+        const uint32_t m = WS == 32 ? 0xffffffffu : (((1u << WS) - 1u) << sh);
+        a = nz1[warp] & m;
+        b = nz2[warp] & m;
+    } else {
+        const int w0 = (wl * WS) >> 5;
+#pragma unroll
+        for (int q = 0; q < WS / 32; ++q) {
+            a |= nz1[w0 + q];
+            b |= nz2[w0 + q];
+        }
+    }
+    return a == 0u || b == 0u;
+}
+
 template <int WS>
 struct TcShape {
     static constexpr int KK = 2 * WS;                          // K (and N) extent: re | im
@@ -188,6 +210,10 @@ __global__ void __launch_bounds__(TcShape<WS>::THREADS, 1) xcorr_tc_kernel(const
     extern __shared__ __align__(1024) uint8_t smem[];
     __shared__ __align__(8) uint64_t mbar[NG];
     __shared__ uint32_t tmem_base;
+    // per warp of each warpgroup: ballots of its pass-A rows holding a nonzero frame-1 /
+    // frame-2 pixel (a window with either frame all zero correlates to exactly 0 in the
+    // reference; its cross spectrum and plane are set to 0 here)
+    __shared__ uint32_t s_nz1[NG][4], s_nz2[NG][4];
 
     const GridGeom &g = a.g;
     const int tid = threadIdx.x, wg = tid >> 7, lt = tid & 127;
@@ -270,6 +296,17 @@ __global__ void __launch_bounds__(TcShape<WS>::THREADS, 1) xcorr_tc_kernel(const
 #pragma unroll
                 for (int i = 0; i < WS; ++i) v1[i] = v2[i] = 0.f;
             }
+            bool nz1 = false, nz2 = false;
+#pragma unroll
+            for (int i = 0; i < WS; ++i) {
+                nz1 |= v1[i] != 0.f;
+                nz2 |= v2[i] != 0.f;
+            }
+            const uint32_t b1 = __ballot_sync(0xffffffffu, nz1), b2 = __ballot_sync(0xffffffffu, nz2);
+            if (lane == 0) {
+                s_nz1[wg][wq] = b1;
+                s_nz2[wg][wq] = b2;
+            }
 #pragma unroll
             for (int c = 0; c < WS / 8; ++c) {
                 store8<NPROD, F16>(a_hi, a_lo, tc::off_kmajor(lt, 8 * c, 128), v1 + 8 * c);
@@ -314,6 +351,7 @@ __global__ void __launch_bounds__(TcShape<WS>::THREADS, 1) xcorr_tc_kernel(const
         }
 
         // ---- cross spectrum; pass C operand: K-major row (wl, kx), k = (re|im, ky) ----
+        const bool dead = window_dead<WS>(s_nz1[wg], s_nz2[wg], wl);
         {
             const bool ok = wait_pass();
             if (ok) {
@@ -329,8 +367,8 @@ __global__ void __launch_bounds__(TcShape<WS>::THREADS, 1) xcorr_tc_kernel(const
                         const int ky = 8 * c + i, km = (WS - ky) % WS;
                         const float pr = __shfl_sync(0xffffffffu, zr[km], partner);
                         const float pi = __shfl_sync(0xffffffffu, zi[km], partner);
-                        cr[i] = 0.5f * (zr[ky] * pi + zi[ky] * pr);
-                        ci[i] = 0.25f * ((pr * pr + pi * pi) - (zr[ky] * zr[ky] + zi[ky] * zi[ky]));
+                        cr[i] = dead ? 0.f : 0.5f * (zr[ky] * pi + zi[ky] * pr);
+                        ci[i] = dead ? 0.f : 0.25f * ((pr * pr + pi * pi) - (zr[ky] * zr[ky] + zi[ky] * zi[ky]));
                     }
                     store8s<NPROD, F16>(a_hi, a_lo, tc::off_kmajor(lt, 8 * c, 128), cr, sC);
                     store8s<NPROD, F16>(a_hi, a_lo, tc::off_kmajor(lt, WS + 8 * c, 128), ci, sC);
@@ -379,7 +417,9 @@ __global__ void __launch_bounds__(TcShape<WS>::THREADS, 1) xcorr_tc_kernel(const
                 tc::tmem_wait_ld();
                 float *prow = planes + wl * (WS * LDF) + ((r + WS / 2) % WS) * LDF;
 #pragma unroll
-                for (int x = 0; x < WS; ++x) prow[(x + WS / 2) % WS] = fabsf(cv[x]) * out_scale;
+                const float k = dead ? 0.f : out_scale;
+#pragma unroll
+                for (int x = 0; x < WS; ++x) prow[(x + WS / 2) % WS] = fabsf(cv[x]) * k;
             }
             tc::fence_before_sync();
             const bool bad = tc::named_sync_or(bar_id, 128, !ok);

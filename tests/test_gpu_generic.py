@@ -172,6 +172,12 @@ def test_generic_against_reference(cuda, wx, wy, nps):
     assert ok.mean() > 0.5
     assert np.array_equal(idx[ok], ri[ok])
     same = (idx == ri) & ok[:, None]
+    for w, q in zip(*np.nonzero(same & (v != rvalid))):
+        li = idx[w, q]
+        fl = planes[w].ravel()
+        nb = [fl[li + o] if 0 <= li + o < fl.size else None for o in (-1, 1, -wx, wx)]
+        print(f"  window {w} peak {q} idx {li}: engine valid {v[w, q]} dx {dx[w, q]} dy {dy[w, q]} val {val[w, q]}; "
+              f"reference valid {rvalid[w, q]} dx {rdx[w, q]} dy {rdy[w, q]} val {rv[w, q]}; neighbours {nb}")
     assert np.array_equal(v[same], rvalid[same])
     both = same & (v == 1)
     tx, ty = fit_tolerance(planes, idx, wx)
