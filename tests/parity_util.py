@@ -79,3 +79,21 @@ def fit_tolerance(planes, idx, wsx, rel_cc=1e-5, base=1e-3, safety=1.0):
         t[undetermined] = np.inf
         out.append(t)
     return out
+
+
+def fit_undetermined(planes, idx, wsx, rel=1e-5):
+    """Candidates whose 3-point fit reads a value within rel (of the window's largest
+    value) of zero: the log of a value at the planes' error level may be finite on one side
+    and -inf on the other, so the fit's validity is not determined by the inputs."""
+    n = planes.shape[0]
+    flat = planes.reshape(n, -1)
+    size = flat.shape[1]
+    tol = rel * flat.max(1)[:, None]
+    out = np.zeros(idx.shape, bool)
+    for o in (0, -1, 1, -wsx, wsx):
+        j = idx + o
+        inside = (idx >= 0) & (j >= 0) & (j < size)
+        val = np.take_along_axis(flat, np.where(inside, j, 0), 1)
+        out |= inside & (val <= tol)
+    return out
+

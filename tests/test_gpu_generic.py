@@ -14,8 +14,9 @@ planes above 20,480 points in a global workspace (256x256, 148x148).  Checked ag
     of the peak, peak indices exact outside near ties, displacements within the fit bound
     for planes that agree to 2e-6;
   - the reference engine itself (oracle/_ref): peak indices exact outside slot overflow and
-    near ties, raw displacements within the fit tolerance, on a pass staged with the
-    reference's own predictor.
+    near ties, validity exact where the fit reads no value within the plane error of zero,
+    raw displacements within the fit tolerance, on a pass staged with the reference's own
+    predictor.
 """
 import numpy as np
 import pytest
@@ -23,7 +24,7 @@ import pytest
 import piv_b200 as P
 from oracle import oracle as O
 from oracle import ref as R
-from parity_util import fit_tolerance, near_ties
+from parity_util import fit_tolerance, fit_undetermined, near_ties
 
 pytestmark = pytest.mark.gpu
 
@@ -171,7 +172,7 @@ def test_generic_against_reference(cuda, wx, wy, nps):
           f"{tie_top.mean():.2%}")
     assert ok.mean() > 0.5
     assert np.array_equal(idx[ok], ri[ok])
-    same = (idx == ri) & ok[:, None]
+    same = (idx == ri) & ok[:, None] & ~fit_undetermined(planes, idx, wx)
     for w, q in zip(*np.nonzero(same & (v != rvalid))):
         li = idx[w, q]
         fl = planes[w].ravel()

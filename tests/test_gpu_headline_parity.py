@@ -38,7 +38,7 @@ import pytest
 
 import piv_b200 as P
 from oracle import ref as R
-from parity_util import fit_tolerance, near_ties
+from parity_util import fit_tolerance, fit_undetermined, near_ties
 
 pytestmark = pytest.mark.gpu
 
@@ -143,7 +143,7 @@ def test_last_pass_peaks_and_candidates(run, k):
     okc = ~tie_cnt
     print(f"grid {k + 1}: counts compared in {okc.mean():.3%} of windows")
     assert np.array_equal(cnt[okc], rc[okc])
-    same = (idx == ri) & ok[:, None]
+    same = (idx == ri) & ok[:, None] & ~fit_undetermined(planes, idx, wsx)
     assert np.array_equal(v[same], rvalid[same])
     both = same & (v == 1)
     tx, ty = fit_tolerance(planes, idx, wsx)
