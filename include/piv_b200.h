@@ -287,8 +287,8 @@ int piv_xcorr_config(const piv_engine *e, int grid, int *windows_per_cta, int *t
  * PIV_XCORR_TC_SPLIT_F16 / PIV_XCORR_TC_F16: the same with FP16 operands (about 22
  * significant bits per split operand, 11 for one product; the passes' operands are scaled
  * by exact powers of two that keep them in FP16's range).  The tensor-core paths cover
- * square 16x16, 32x32 and 64x64 windows with up to 8 saved peaks (PIV_ERR_UNSUPPORTED
- * otherwise).  PIV_XCORR_PATH=tc|tc1|tch|tch1 in the environment at piv_create selects
+ * 16x16, 32x32, 64x64, 48x24 and 24x48 windows with up to 8 saved peaks
+ * (PIV_ERR_UNSUPPORTED otherwise).  PIV_XCORR_PATH=tc|tc1|tch|tch1 in the environment at piv_create selects
  * them for every grid they cover. */
 #define PIV_XCORR_SIMT 0
 #define PIV_XCORR_TC_SPLIT 1

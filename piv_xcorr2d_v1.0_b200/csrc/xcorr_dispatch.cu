@@ -219,7 +219,21 @@ PIV_TC(32)
 PIV_TC(64)
 #undef PIV_TC
 
-bool xcorr_tc_supported(int wsx, int wsy) { return wsx == wsy && (wsx == 16 || wsx == 32 || wsx == 64); }
+template <int WX, int WY, int NPROD, bool F16>
+cudaError_t launch_tc_rect_shape(const XcorrArgs &a, bool deformed, int K, cudaStream_t s);
+#define PIV_TCR(WX, WY) \
+    extern template cudaError_t launch_tc_rect_shape<WX, WY, 3, false>(const XcorrArgs &, bool, int, cudaStream_t); \
+    extern template cudaError_t launch_tc_rect_shape<WX, WY, 1, false>(const XcorrArgs &, bool, int, cudaStream_t); \
+    extern template cudaError_t launch_tc_rect_shape<WX, WY, 3, true>(const XcorrArgs &, bool, int, cudaStream_t); \
+    extern template cudaError_t launch_tc_rect_shape<WX, WY, 1, true>(const XcorrArgs &, bool, int, cudaStream_t);
+PIV_TCR(48, 24)
+PIV_TCR(24, 48)
+#undef PIV_TCR
+
+bool xcorr_tc_supported(int wsx, int wsy)
+{
+    return (wsx == wsy && (wsx == 16 || wsx == 32 || wsx == 64)) || (wsx == 48 && wsy == 24) || (wsx == 24 && wsy == 48);
+}
 
 cudaError_t launch_xcorr_tc(const XcorrArgs &a, bool deformed, cudaStream_t s, const char **why, int nprod, bool f16)
 {
@@ -237,6 +251,17 @@ cudaError_t launch_xcorr_tc(const XcorrArgs &a, bool deformed, cudaStream_t s, c
         if (f16) return nprod == 3 ? launch_tc_shape<WS, 3, true>(a, deformed, K, s) : launch_tc_shape<WS, 1, true>(a, deformed, K, s);
         return nprod == 3 ? launch_tc_shape<WS, 3, false>(a, deformed, K, s) : launch_tc_shape<WS, 1, false>(a, deformed, K, s);
     };
+    if (a.g.ws_x != a.g.ws_y) {
+        auto rect = [&](auto wx, auto wy) -> cudaError_t {
+            constexpr int WX = decltype(wx)::value, WY = decltype(wy)::value;
+            if (f16) return nprod == 3 ? launch_tc_rect_shape<WX, WY, 3, true>(a, deformed, K, s)
+                                       : launch_tc_rect_shape<WX, WY, 1, true>(a, deformed, K, s);
+            return nprod == 3 ? launch_tc_rect_shape<WX, WY, 3, false>(a, deformed, K, s)
+                              : launch_tc_rect_shape<WX, WY, 1, false>(a, deformed, K, s);
+        };
+        if (a.g.ws_x == 48) return rect(std::integral_constant<int, 48>{}, std::integral_constant<int, 24>{});
+        return rect(std::integral_constant<int, 24>{}, std::integral_constant<int, 48>{});
+    }
     if (a.g.ws_x == 16) return pick(std::integral_constant<int, 16>{});
     if (a.g.ws_x == 32) return pick(std::integral_constant<int, 32>{});
     return pick(std::integral_constant<int, 64>{});

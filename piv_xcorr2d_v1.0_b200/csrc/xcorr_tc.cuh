@@ -416,7 +416,6 @@ __global__ void __launch_bounds__(TcShape<WS>::THREADS, 1) xcorr_tc_kernel(const
                 tmem_row<WS>(lane_addr, cv);
                 tc::tmem_wait_ld();
                 float *prow = planes + wl * (WS * LDF) + ((r + WS / 2) % WS) * LDF;
-#pragma unroll
                 const float k = dead ? 0.f : out_scale;
 #pragma unroll
                 for (int x = 0; x < WS; ++x) prow[(x + WS / 2) % WS] = fabsf(cv[x]) * k;

@@ -97,7 +97,7 @@ def test_precision_sweep(frames, monkeypatch, wx, wy):
     rows = []
     for name, path, generic in PATHS:
         tc = path != P.PIV_XCORR_SIMT
-        if tc and not (wx == wy and wx in (16, 32, 64)):
+        if tc and not ((wx == wy and wx in (16, 32, 64)) or (wx, wy) in ((48, 24), (24, 48))):
             rows.append((name, None))
             continue
         planes, (cnt, idx, val), (_, _, dx, dy, v), geom = _run(p, f1, f2, path, generic, monkeypatch)
