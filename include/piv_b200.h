@@ -289,7 +289,9 @@ int piv_xcorr_config(const piv_engine *e, int grid, int *windows_per_cta, int *t
  * by exact powers of two that keep them in FP16's range).  The tensor-core paths cover
  * 16x16, 32x32, 64x64, 48x24 and 24x48 windows with up to 8 saved peaks
  * (PIV_ERR_UNSUPPORTED otherwise).  PIV_XCORR_PATH=tc|tc1|tch|tch1 in the environment at piv_create selects
- * them for every grid they cover. */
+ * them for every grid they cover.  At 16x16 and 32x32 with spacing up to half the window,
+ * a tile's windows of one grid row are staged into shared memory by TMA tensor-map copies
+ * (identical results to direct loads; PIV_TC_STAGING=0 at piv_create turns it off). */
 #define PIV_XCORR_SIMT 0
 #define PIV_XCORR_TC_SPLIT 1
 #define PIV_XCORR_TC_BF16 2

@@ -144,6 +144,11 @@ struct GridState {
     int gws_ctas = 0;
     float tuned_ms[8] = {};   // measured time per variant (0 = not measured)
     int n_tuned = 0;
+    // TMA staging maps of the tensor-core kernels, built at their first launch (the frame and
+    // deformed-frame buffers live as long as the engine): [0] the undeformed pass, [1] the
+    // deformed pass
+    TcStaging stage[2];
+    bool stage_built[2] = {false, false};
 };
 
 struct piv_engine {
@@ -156,6 +161,7 @@ struct piv_engine {
     uint8_t *d_stage1 = nullptr, *d_stage2 = nullptr;
     uint8_t *d_f1 = nullptr, *d_f2 = nullptr;
     int mx = 0, my = 0, pitch = 0, rows = 0;
+    bool tc_staging = true;  // tensor-core kernels stage window rows through TMA where they can
     GridState grid[2];
     MheGeom mg{};
     int *d_levels = nullptr;
@@ -417,7 +423,17 @@ int do_xcorr(piv_engine *e, int k, bool deformed, int first, int end, float *dum
         if (gs.path == PIV_XCORR_SIMT) return launch_xcorr(a, deformed, e->stream, &why, gs.variant);
         const bool split = gs.path == PIV_XCORR_TC_SPLIT || gs.path == PIV_XCORR_TC_SPLIT_F16;
         const bool f16 = gs.path == PIV_XCORR_TC_SPLIT_F16 || gs.path == PIV_XCORR_TC_F16;
-        return launch_xcorr_tc(a, deformed, e->stream, &why, split ? 3 : 1, f16);
+        const TcStaging *stage = nullptr;
+        if (gs.gg.ws_x == gs.gg.ws_y && e->tc_staging) {
+            const int d = deformed ? 1 : 0;
+            if (!gs.stage_built[d]) {
+                tc_staging_build(gs.stage[d], gs.gg.ws_x, gs.gg.sp_x, e->d_f1, e->d_f2, e->pitch, e->rows,
+                                 deformed ? gs.def : nullptr, gs.def_pitch, gs.gg.Ny_aug);
+                gs.stage_built[d] = true;
+            }
+            stage = &gs.stage[d];
+        }
+        return launch_xcorr_tc(a, deformed, e->stream, &why, split ? 3 : 1, f16, stage);
     };
     if (dump) {
         a.w_first = first;
@@ -762,6 +778,7 @@ int piv_create(const piv_params *p, piv_engine **out)
         return bail(set_err(e, PIV_ERR_CUDA, "stream creation failed"));
     if (const char *v = getenv("PIV_TEST_FAIL_ALLOC")) e->fail_alloc_at = atoi(v);
     if (const char *v = getenv("PIV_TEST_FILL_CAP")) e->fill_cap = atoi(v);
+    if (const char *v = getenv("PIV_TC_STAGING")) e->tc_staging = atoi(v) != 0;  // 0: direct row loads
     // frame padding: every window of both grids reads inside the buffer
     int mx = 0, my = 0;
     const int wsx[2] = {p->ws_x1, p->ws_x2}, wsy[2] = {p->ws_y1, p->ws_y2};

@@ -2,6 +2,7 @@
 // argument blocks, compile-time twiddle generation.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -155,8 +156,22 @@ int xcorr_variants(int ws_x, int ws_y);
 bool xcorr_variant_shape(int ws_x, int ws_y, int variant, int *windows_per_cta, int *threads_per_cta);
 // Tensor-core path (xcorr_tc.cuh): nprod 3 = split-BF16 (hi*hi + hi*lo + lo*hi), 1 = BF16.
 bool xcorr_tc_supported(int ws_x, int ws_y);
+// TMA staging of the tiles' rows (tensor-core kernels of 16 and 32 px windows): 2D tensor
+// maps of frame 1 (u8) and of frame 2 (the u8 frame for an undeformed pass, the FP32 deformed
+// frame otherwise), their boxes' widths in elements (frame 1, frame 2), and whether to use
+// them (tc_staging_build sets use = 0 where the boxes do not fit the kernel's buffers).
+struct TcStaging {
+    CUtensorMap f1, f2;
+    int bx1, bx2;
+    int use;
+};
+// Encodes the maps for square WS x WS windows at spacing sp_x (box: a tile's 128/WS windows
+// of one grid row, x rounded down to 16 bytes): frames f1, f2 of `pitch` x `rows` bytes,
+// deformed frame `def` of def_pitch x def_rows floats (NULL: the undeformed form).
+cudaError_t tc_staging_build(TcStaging &st, int ws, int sp_x, const uint8_t *f1, const uint8_t *f2, int pitch,
+                             int rows, const float *def, int def_pitch, int def_rows);
 cudaError_t launch_xcorr_tc(const XcorrArgs &a, bool deformed, cudaStream_t s, const char **why, int nprod,
-                            bool f16);
+                            bool f16, const TcStaging *stage);
 
 // Field kernels (field_kernels.cu).
 struct DeformArgs {

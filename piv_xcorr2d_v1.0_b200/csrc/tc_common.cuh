@@ -103,6 +103,24 @@ __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity)
     return false;
 }
 
+// --- TMA (bulk tensor copies, global -> shared) -------------------------------------
+// Arm an mbarrier for `bytes` of incoming transactions (one arrival by the calling thread).
+__device__ __forceinline__ void mbar_expect_tx(uint32_t mbar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar), "r"(bytes) : "memory");
+}
+
+// 2D tile load of the tensor map's box at (x, y) (x: innermost coordinate, already a multiple
+// of 16 bytes) into shared memory at dst (128-byte aligned); completion counted on mbar.  No
+// multicast.  Out-of-range parts of the box read zero.
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const void *tmap, int x, int y, uint32_t mbar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(tmap)), "r"(x), "r"(y), "r"(mbar)
+        : "memory");
+}
+
 // --- named barriers (one per warpgroup; barrier 0 is __syncthreads) -------------
 __device__ __forceinline__ void named_sync(uint32_t id, uint32_t nthreads)
 {

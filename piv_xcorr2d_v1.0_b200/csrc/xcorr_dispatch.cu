@@ -2,6 +2,7 @@
 // Every shape (WSX, WSY) is compiled in its own translation unit (xcorr_shape_*.cu) in
 // several variants (B windows per CTA, NT threads per CTA); the first listed variant of a
 // shape is its default, the engine's autotuner may pick another one per grid.
+#include <cstring>
 #include <type_traits>
 
 #include "piv_common.cuh"
@@ -208,12 +209,12 @@ cudaError_t launch_xcorr(const XcorrArgs &a, bool deformed, cudaStream_t s, cons
 namespace piv {
 
 template <int WS, int NPROD, bool F16>
-cudaError_t launch_tc_shape(const XcorrArgs &a, bool deformed, int K, cudaStream_t s);
+cudaError_t launch_tc_shape(const XcorrArgs &a, bool deformed, int K, cudaStream_t s, const TcStaging *stage);
 #define PIV_TC(WS) \
-    extern template cudaError_t launch_tc_shape<WS, 3, false>(const XcorrArgs &, bool, int, cudaStream_t); \
-    extern template cudaError_t launch_tc_shape<WS, 1, false>(const XcorrArgs &, bool, int, cudaStream_t); \
-    extern template cudaError_t launch_tc_shape<WS, 3, true>(const XcorrArgs &, bool, int, cudaStream_t); \
-    extern template cudaError_t launch_tc_shape<WS, 1, true>(const XcorrArgs &, bool, int, cudaStream_t);
+    extern template cudaError_t launch_tc_shape<WS, 3, false>(const XcorrArgs &, bool, int, cudaStream_t, const TcStaging *); \
+    extern template cudaError_t launch_tc_shape<WS, 1, false>(const XcorrArgs &, bool, int, cudaStream_t, const TcStaging *); \
+    extern template cudaError_t launch_tc_shape<WS, 3, true>(const XcorrArgs &, bool, int, cudaStream_t, const TcStaging *); \
+    extern template cudaError_t launch_tc_shape<WS, 1, true>(const XcorrArgs &, bool, int, cudaStream_t, const TcStaging *);
 PIV_TC(16)
 PIV_TC(32)
 PIV_TC(64)
@@ -235,7 +236,63 @@ bool xcorr_tc_supported(int wsx, int wsy)
     return (wsx == wsy && (wsx == 16 || wsx == 32 || wsx == 64)) || (wsx == 48 && wsy == 24) || (wsx == 24 && wsy == 48);
 }
 
-cudaError_t launch_xcorr_tc(const XcorrArgs &a, bool deformed, cudaStream_t s, const char **why, int nprod, bool f16)
+namespace {
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_tiled()
+{
+    static EncodeTiledFn fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &f, 12000, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(f);
+    }
+    return fn;
+}
+
+// a 2D map of a [rows][width] buffer (row stride `stride` bytes), box {bx, by}, zero fill
+bool encode_2d(CUtensorMap &m, CUtensorMapDataType type, const void *base, int width, int rows, size_t stride, int bx,
+               int by)
+{
+    EncodeTiledFn fn = encode_tiled();
+    if (!fn || !base || (reinterpret_cast<uintptr_t>(base) & 15) || (stride & 15)) return false;
+    const cuuint64_t dims[2] = {(cuuint64_t)width, (cuuint64_t)rows};
+    const cuuint64_t strides[1] = {(cuuint64_t)stride};
+    const cuuint32_t box[2] = {(cuuint32_t)bx, (cuuint32_t)by};
+    const cuuint32_t estr[2] = {1, 1};
+    return fn(&m, type, 2, const_cast<void *>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+              CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+}  // namespace
+
+cudaError_t tc_staging_build(TcStaging &st, int ws, int sp_x, const uint8_t *f1, const uint8_t *f2, int pitch,
+                             int rows, const float *def, int def_pitch, int def_rows)
+{
+    memset(&st, 0, sizeof(st));
+    if (ws != 16 && ws != 32) return cudaSuccess;  // 64 px windows load their rows directly
+    const int nwin = 128 / ws, span = (nwin - 1) * sp_x + ws;
+    st.bx1 = (span + 15 + 15) / 16 * 16;  // + up to 15 bytes of rounding the box start down
+    st.bx2 = (span + 3 + 3) / 4 * 4;      // + up to 3 floats
+    if (st.bx1 > 128 || st.bx2 > 128) return cudaSuccess;  // the kernel's staging buffers
+    if (!encode_2d(st.f1, CU_TENSOR_MAP_DATA_TYPE_UINT8, f1, pitch, rows, (size_t)pitch, st.bx1, ws))
+        return cudaSuccess;
+    const bool ok = def ? encode_2d(st.f2, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, def, def_pitch, def_rows,
+                                    (size_t)def_pitch * sizeof(float), st.bx2, ws)
+                        : encode_2d(st.f2, CU_TENSOR_MAP_DATA_TYPE_UINT8, f2, pitch, rows, (size_t)pitch, st.bx1, ws);
+    st.use = ok ? 1 : 0;
+    return cudaSuccess;
+}
+
+cudaError_t launch_xcorr_tc(const XcorrArgs &a, bool deformed, cudaStream_t s, const char **why, int nprod, bool f16,
+                            const TcStaging *stage)
 {
     if (a.g.Nps > 8) {
         if (why) *why = "Npeak_save > 8 is not built into this engine";
@@ -248,8 +305,10 @@ cudaError_t launch_xcorr_tc(const XcorrArgs &a, bool deformed, cudaStream_t s, c
     const int K = a.g.Nps <= 4 ? 4 : 8;
     auto pick = [&](auto ws) -> cudaError_t {
         constexpr int WS = decltype(ws)::value;
-        if (f16) return nprod == 3 ? launch_tc_shape<WS, 3, true>(a, deformed, K, s) : launch_tc_shape<WS, 1, true>(a, deformed, K, s);
-        return nprod == 3 ? launch_tc_shape<WS, 3, false>(a, deformed, K, s) : launch_tc_shape<WS, 1, false>(a, deformed, K, s);
+        if (f16) return nprod == 3 ? launch_tc_shape<WS, 3, true>(a, deformed, K, s, stage)
+                                   : launch_tc_shape<WS, 1, true>(a, deformed, K, s, stage);
+        return nprod == 3 ? launch_tc_shape<WS, 3, false>(a, deformed, K, s, stage)
+                          : launch_tc_shape<WS, 1, false>(a, deformed, K, s, stage);
     };
     if (a.g.ws_x != a.g.ws_y) {
         auto rect = [&](auto wx, auto wy) -> cudaError_t {

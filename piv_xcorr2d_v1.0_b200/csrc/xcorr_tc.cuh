@@ -34,6 +34,10 @@
 // Waits on the MMA completion barrier are bounded: on a timeout the warpgroup stops,
 // sets bit kStatusMmaWait in *a.status, and the CTA releases its tensor memory.
 #pragma once
+#include <cuda.h>
+
+#include <cstring>
+
 #include "tc_common.cuh"
 #include "xcorr_kernel.cuh"
 
@@ -91,6 +95,47 @@ __device__ __forceinline__ void store8s(uint8_t *hi, uint8_t *lo, uint32_t off, 
 #pragma unroll
     for (int i = 0; i < 8; ++i) w[i] = v[i] * scale;
     store8<NPROD, F16>(hi, lo, off, w);
+}
+
+// A staged row of W bytes at any byte offset in shared memory: the aligned words covering
+// it, each output word assembled by a funnel shift (reads up to 3 bytes past the row, inside
+// the staging region), bytes converted as in load_u8_row.
+template <int W>
+__device__ __forceinline__ void load_u8_row_shared(const uint8_t *p, float (&v)[W])
+{
+    static_assert(W % 4 == 0, "rows of whole words");
+    const uintptr_t ad = reinterpret_cast<uintptr_t>(p);
+    const uint32_t *q = reinterpret_cast<const uint32_t *>(ad & ~(uintptr_t)3);
+    const uint32_t sh = (uint32_t)(ad & 3) * 8;
+    uint32_t w[W / 4 + 1];
+#pragma unroll
+    for (int i = 0; i <= W / 4; ++i) w[i] = q[i];
+#pragma unroll
+    for (int c = 0; c < W / 4; ++c) {
+        const uint32_t u = __funnelshift_r(w[c], w[c + 1], sh);
+        v[4 * c + 0] = byte_to_float<0>(u);
+        v[4 * c + 1] = byte_to_float<1>(u);
+        v[4 * c + 2] = byte_to_float<2>(u);
+        v[4 * c + 3] = byte_to_float<3>(u);
+    }
+}
+
+template <int W>
+__device__ __forceinline__ void load_f32_row_shared(const float *p, float (&v)[W])
+{
+    if ((reinterpret_cast<uintptr_t>(p) & 15) == 0) {
+#pragma unroll
+        for (int q = 0; q < W / 4; ++q) {
+            const float4 u = reinterpret_cast<const float4 *>(p)[q];
+            v[4 * q] = u.x;
+            v[4 * q + 1] = u.y;
+            v[4 * q + 2] = u.z;
+            v[4 * q + 3] = u.w;
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < W; ++i) v[i] = p[i];
+    }
 }
 
 // One pass: D[128 x N] = A[128 x KK] * B^T over KK/16 K steps.  A in the K-major
@@ -188,11 +233,20 @@ struct TcShape {
     static constexpr uint32_t G_BYTES = KK * KK * 2;            // one of G hi / lo
     static constexpr uint32_t A_BYTES = 128 * KK * 2;           // one of A hi / lo
     static constexpr int TCOLS = KK < 32 ? 32 : KK;             // TMEM columns per warpgroup
-    static constexpr size_t SMEM = 2 * (size_t)G_BYTES + (size_t)NG * 2 * A_BYTES;
+    static constexpr size_t BASE = 2 * (size_t)G_BYTES + (size_t)NG * 2 * A_BYTES;
+    // TMA staging of a tile's rows per warpgroup (16 and 32 px windows; 64 px windows have no
+    // shared memory left and load their rows directly): frame-1 box of up to kStageBx bytes per
+    // row, frame-2 box of up to kStageBx floats per row
+    static constexpr int STAGE_BX = WS <= 32 ? 128 : 0;
+    static constexpr uint32_t STAGE1 = WS * STAGE_BX, STAGE2 = WS * STAGE_BX * 4;
+    static constexpr size_t SMEM = BASE + (size_t)NG * (STAGE1 + STAGE2);
+    static_assert(SMEM <= 232448, "shared memory");
 };
 
+
 template <int WS, int NPROD, int K, bool DEF, bool F16>
-__global__ void __launch_bounds__(TcShape<WS>::THREADS, 1) xcorr_tc_kernel(const XcorrArgs a)
+__global__ void __launch_bounds__(TcShape<WS>::THREADS, 1) xcorr_tc_kernel(const XcorrArgs a,
+                                                                           const __grid_constant__ TcStaging st)
 {
     using S = TcShape<WS>;
     constexpr int KK = S::KK, NG = S::NG;
@@ -209,6 +263,7 @@ __global__ void __launch_bounds__(TcShape<WS>::THREADS, 1) xcorr_tc_kernel(const
 
     extern __shared__ __align__(1024) uint8_t smem[];
     __shared__ __align__(8) uint64_t mbar[NG];
+    __shared__ __align__(8) uint64_t mbar_tma[NG];
     __shared__ uint32_t tmem_base;
     // per warp of each warpgroup: ballots of its pass-A rows holding a nonzero frame-1 /
     // frame-2 pixel (a window with either frame all zero correlates to exactly 0 in the
@@ -224,6 +279,11 @@ __global__ void __launch_bounds__(TcShape<WS>::THREADS, 1) xcorr_tc_kernel(const
     float *planes = reinterpret_cast<float *>(a_hi);
     const uint32_t mb = tc::smem_u32(&mbar[wg]);
     const uint32_t bar_id = 1 + wg;
+    uint8_t *stg1 = smem + S::BASE + (size_t)wg * (S::STAGE1 + S::STAGE2), *stg2 = stg1 + S::STAGE1;
+    const uint32_t mbt = tc::smem_u32(&mbar_tma[wg]);
+    // (TMA writes need 128-byte aligned destinations: the staging region is placed at a
+    // multiple of 1024 bytes from a dynamic-shared-memory base the kernel checks here)
+    const bool use_tma = S::STAGE_BX > 0 && st.use != 0 && (tc::smem_u32(smem + S::BASE) & 1023u) == 0;
 
     // DFT matrix G = [[C, -S], [S, C]], hi/lo, in the shared layout buf(r, c)
     for (int t = tid; t < KK * KK; t += S::THREADS) {
@@ -240,6 +300,7 @@ __global__ void __launch_bounds__(TcShape<WS>::THREADS, 1) xcorr_tc_kernel(const
     }
     if (lt == 0) {
         tc::mbar_init(mb, 1);
+        tc::mbar_init(mbt, 1);
         tc::fence_mbar_init();
     }
     if (tid < 32) tc::tmem_alloc(tc::smem_u32(&tmem_base), TALLOC);
@@ -276,13 +337,72 @@ __global__ void __launch_bounds__(TcShape<WS>::THREADS, 1) xcorr_tc_kernel(const
         return !bad;
     };
 
+    // TMA staging: a tile is staged when its NWIN windows lie in one row of the window grid;
+    // the box starts at the tile's first window, x rounded down to a 16-byte boundary
+    uint32_t tphase = 0;
+    int tma_pending = 0;
+    auto in_row = [&](int tile) -> bool {
+        const int w0 = a.w_first + tile * NWIN;
+        return use_tma && (w0 % g.Nx_vec) + NWIN <= g.Nx_vec;
+    };
+    auto tile_x = [&](int tile, int &iy, int &ix0, int &x1, int &y1, int &x2) {
+        const int w0 = a.w_first + tile * NWIN;
+        iy = w0 / g.Nx_vec;
+        ix0 = w0 - iy * g.Nx_vec;
+        x1 = ix0 * g.sp_x - g.Nx_left + a.f1.mx;  // frame column of window 0 (padded frame)
+        y1 = iy * g.sp_y - g.Ny_left + a.f1.my;
+        x2 = ix0 * g.sp_x;                         // deformed-frame column of window 0
+    };
+    auto issue_stage = [&](int tile) {  // one thread
+        int iy, ix0, x1, y1, x2;
+        tile_x(tile, iy, ix0, x1, y1, x2);
+        const int xa1 = x1 & ~15;
+        const uint32_t bytes = (uint32_t)st.bx1 * WS + (DEF ? (uint32_t)st.bx2 * 4 * WS : (uint32_t)st.bx1 * WS);
+        tc::mbar_expect_tx(mbt, bytes);
+        tc::tma_load_2d(tc::smem_u32(stg1), &st.f1, xa1, y1, mbt);
+        if constexpr (DEF) tc::tma_load_2d(tc::smem_u32(stg2), &st.f2, x2 & ~3, iy * g.sp_y, mbt);
+        else tc::tma_load_2d(tc::smem_u32(stg2), &st.f2, xa1, y1, mbt);
+    };
+    {
+        const int first = blockIdx.x * NG + wg;
+        if (first < n_tiles && in_row(first)) {
+            if (lt == 0) issue_stage(first);
+            ++tma_pending;
+        }
+    }
+
     for (int tile = blockIdx.x * NG + wg; tile < n_tiles; tile += gridDim.x * NG) {
         const int w = a.w_first + tile * NWIN + wl;
+        const bool staged = in_row(tile);
+        bool ok_rows = true;
 
         // ---- pass A operand: row (wl, y = r) = [f1 row | f2 row], K-major ----
         {
             float v1[WS], v2[WS];
-            if (w < a.w_end) {
+            if (staged) {
+                // a copy that did not land in time stays pending (same phase) for the exit path
+                ok_rows = __all_sync(0xffffffffu, tc::mbar_wait(mbt, tphase & 1));
+                if (ok_rows) {
+                    ++tphase;
+                    --tma_pending;
+                }
+            }
+            if (staged && ok_rows) {
+                int iy, ix0, x1, y1, x2;
+                tile_x(tile, iy, ix0, x1, y1, x2);
+                const uint8_t *row1 = stg1 + r * st.bx1 + (x1 - (x1 & ~15)) + wl * g.sp_x;
+                load_u8_row_shared<WS>(row1, v1);
+                if constexpr (DEF) {
+                    const float *row2 = reinterpret_cast<const float *>(stg2) + r * st.bx2 + (x2 - (x2 & ~3)) + wl * g.sp_x;
+                    load_f32_row_shared<WS>(row2, v2);
+                } else {
+                    load_u8_row_shared<WS>(stg2 + r * st.bx1 + (x1 - (x1 & ~15)) + wl * g.sp_x, v2);
+                }
+                if (w >= a.w_end) {  // a partial last tile: windows past the launch read nothing
+#pragma unroll
+                    for (int i = 0; i < WS; ++i) v1[i] = v2[i] = 0.f;
+                }
+            } else if (!staged && w < a.w_end) {
                 const int iy = w / g.Nx_vec, ix = w - iy * g.Nx_vec;
                 const int x0 = ix * g.sp_x - g.Nx_left + a.f1.mx;
                 const int y1 = iy * g.sp_y + r - g.Ny_left + a.f1.my;
@@ -313,11 +433,21 @@ __global__ void __launch_bounds__(TcShape<WS>::THREADS, 1) xcorr_tc_kernel(const
                 store8<NPROD, F16>(a_hi, a_lo, tc::off_kmajor(lt, WS + 8 * c, 128), v2 + 8 * c);
             }
         }
-        if (!sync_issue(true)) break;
-        if (lt == 0) {
-            // frame 1 is integer-valued (exact in bf16); frame 2 only when deformed
-            issue_pass<KK, KK, false, true, NPROD, DEF ? WS / 16 : KK / 16, F16>(tmem, sa_hi, sa_lo, sg_hi, sg_lo);
-            tc::mma_commit(mb);
+        if (!sync_issue(ok_rows)) {
+            failed = true;
+            break;
+        }
+        {
+            // the staging buffer is consumed: stage the warpgroup's next tile behind this one
+            const int next = tile + gridDim.x * NG;
+            const bool stage_next = next < n_tiles && in_row(next);
+            if (stage_next) ++tma_pending;
+            if (lt == 0) {
+                // frame 1 is integer-valued (exact in bf16); frame 2 only when deformed
+                issue_pass<KK, KK, false, true, NPROD, DEF ? WS / 16 : KK / 16, F16>(tmem, sa_hi, sa_lo, sg_hi, sg_lo);
+                tc::mma_commit(mb);
+                if (stage_next) issue_stage(next);
+            }
         }
 
         // ---- pass B operand: MN-major, m = (wl, position of kx), k = (re|im, y = r) ----
@@ -452,8 +582,10 @@ __global__ void __launch_bounds__(TcShape<WS>::THREADS, 1) xcorr_tc_kernel(const
     if (failed) {
         if (lt == 0 && a.status) atomicOr(a.status, kStatusMmaWait);
         // the pass that did not complete in time gets one more bounded wait before the
-        // tensor memory is released
+        // tensor memory is released, and a staging copy still in flight one before the
+        // shared memory is
         tc::mbar_wait(mb, (phase - 1) & 1);
+        if (tma_pending > 0) tc::mbar_wait(mbt, tphase & 1);
     }
     tc::fence_before_sync();
     __syncthreads();
@@ -463,7 +595,7 @@ __global__ void __launch_bounds__(TcShape<WS>::THREADS, 1) xcorr_tc_kernel(const
 // Launch of one tensor-core shape: one CTA per SM (a kernel using tensor memory is
 // resident once per SM), persistent over the tiles.
 template <int WS, int NPROD, bool F16>
-cudaError_t launch_tc_shape(const XcorrArgs &a, bool deformed, int K, cudaStream_t s)
+cudaError_t launch_tc_shape(const XcorrArgs &a, bool deformed, int K, cudaStream_t s, const TcStaging *stage)
 {
     using S = TcShape<WS>;
     const int n = a.w_end - a.w_first;
@@ -478,7 +610,9 @@ cudaError_t launch_tc_shape(const XcorrArgs &a, bool deformed, int K, cudaStream
         if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return;
         const int want = (tiles + S::NG - 1) / S::NG;
         const int grid = want < sms ? want : sms;
-        kern<<<grid, S::THREADS, S::SMEM, s>>>(a);
+        TcStaging none;
+        memset(&none, 0, sizeof(none));
+        kern<<<grid, S::THREADS, S::SMEM, s>>>(a, stage ? *stage : none);
         e = cudaGetLastError();
     };
     if (K <= 4) {

@@ -2,8 +2,8 @@
 #include "xcorr_tc.cuh"
 
 namespace piv {
-template cudaError_t launch_tc_shape<32, 3, false>(const XcorrArgs &, bool, int, cudaStream_t);
-template cudaError_t launch_tc_shape<32, 3, true>(const XcorrArgs &, bool, int, cudaStream_t);
-template cudaError_t launch_tc_shape<32, 1, false>(const XcorrArgs &, bool, int, cudaStream_t);
-template cudaError_t launch_tc_shape<32, 1, true>(const XcorrArgs &, bool, int, cudaStream_t);
+template cudaError_t launch_tc_shape<32, 3, false>(const XcorrArgs &, bool, int, cudaStream_t, const TcStaging *);
+template cudaError_t launch_tc_shape<32, 3, true>(const XcorrArgs &, bool, int, cudaStream_t, const TcStaging *);
+template cudaError_t launch_tc_shape<32, 1, false>(const XcorrArgs &, bool, int, cudaStream_t, const TcStaging *);
+template cudaError_t launch_tc_shape<32, 1, true>(const XcorrArgs &, bool, int, cudaStream_t, const TcStaging *);
 }  // namespace piv
