@@ -79,23 +79,27 @@ __device__ __forceinline__ void mbar_inval(uint32_t mbar)
     asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(mbar) : "memory");
 }
 
+// One probe: the thread is suspended until the phase completes or kSuspendNs elapse (the
+// suspend-time hint), instead of returning at once, so that waiting warps do not spend issue
+// slots polling while the other warpgroups of the SM work.
+constexpr uint32_t kSuspendNs = 1000000;  // 1 ms
 __device__ __forceinline__ bool mbar_try_wait(uint32_t mbar, uint32_t parity)
 {
     uint32_t done;
     asm volatile(
-        "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+        "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2, %3;\n\t"
         "selp.b32 %0, 1, 0, P1;\n\t}"
         : "=r"(done)
-        : "r"(mbar), "r"(parity)
+        : "r"(mbar), "r"(parity), "r"(kSuspendNs)
         : "memory");
     return done != 0;
 }
 
-// Bounded wait for the phase with the given parity to complete: at most kMaxTries
-// try_wait probes (each suspends for at most a hardware-defined interval), so the
-// wait always ends; false means the phase never completed (the caller records an
-// error and leaves without reading the accumulator).
-constexpr int kMaxTries = 1 << 20;
+// Bounded wait for the phase with the given parity to complete: at most kMaxTries probes
+// of at most kSuspendNs each (about 2 s in all), so the wait always ends; false means the
+// phase never completed (the caller records an error and leaves without reading the
+// accumulator).
+constexpr int kMaxTries = 2048;
 __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity)
 {
     for (int it = 0; it < kMaxTries; ++it)
