@@ -87,14 +87,48 @@ __device__ __forceinline__ void store8(uint8_t *hi, uint8_t *lo, uint32_t off, c
     if constexpr (NPROD > 1) *reinterpret_cast<uint4 *>(lo + off) = l;
 }
 
-// the 8 values scaled by a power of two, then stored as above
-template <int NPROD, bool F16>
+// the 8 values scaled by a power of two (SCALE), then stored as above
+template <int NPROD, bool F16, bool SCALE>
 __device__ __forceinline__ void store8s(uint8_t *hi, uint8_t *lo, uint32_t off, const float *v, float scale)
 {
-    float w[8];
+    if constexpr (SCALE) {
+        float w[8];
 #pragma unroll
-    for (int i = 0; i < 8; ++i) w[i] = v[i] * scale;
-    store8<NPROD, F16>(hi, lo, off, w);
+        for (int i = 0; i < 8; ++i) w[i] = v[i] * scale;
+        store8<NPROD, F16>(hi, lo, off, w);
+    } else {
+        store8<NPROD, F16>(hi, lo, off, v);
+    }
+}
+
+// 8 values exact in the operand type (integers up to 256): the hi part only, the lo part
+// being zero (the MMAs never read it for these K columns)
+template <bool F16>
+__device__ __forceinline__ void store8_exact(uint8_t *hi, uint32_t off, const float *v)
+{
+    uint4 h;
+    if constexpr (F16) {
+        const __half2 a = __floats2half2_rn(v[0], v[1]), b = __floats2half2_rn(v[2], v[3]);
+        const __half2 c = __floats2half2_rn(v[4], v[5]), d = __floats2half2_rn(v[6], v[7]);
+        h = make_uint4(*reinterpret_cast<const uint32_t *>(&a), *reinterpret_cast<const uint32_t *>(&b),
+                       *reinterpret_cast<const uint32_t *>(&c), *reinterpret_cast<const uint32_t *>(&d));
+    } else {
+        const __nv_bfloat162 a = __floats2bfloat162_rn(v[0], v[1]), b = __floats2bfloat162_rn(v[2], v[3]);
+        const __nv_bfloat162 c = __floats2bfloat162_rn(v[4], v[5]), d = __floats2bfloat162_rn(v[6], v[7]);
+        h = make_uint4(*reinterpret_cast<const uint32_t *>(&a), *reinterpret_cast<const uint32_t *>(&b),
+                       *reinterpret_cast<const uint32_t *>(&c), *reinterpret_cast<const uint32_t *>(&d));
+    }
+    *reinterpret_cast<uint4 *>(hi + off) = h;
+}
+
+// whether any of the W values is nonzero (by their bits, sign masked): a 3-input OR tree
+template <int W>
+__device__ __forceinline__ bool any_nonzero(const float (&v)[W])
+{
+    uint32_t acc = 0;
+#pragma unroll
+    for (int i = 0; i < W; ++i) acc |= __float_as_uint(v[i]);
+    return (acc & 0x7fffffffu) != 0u;
 }
 
 // A staged row of W bytes at any byte offset in shared memory: the aligned words covering
@@ -254,10 +288,14 @@ __global__ void __launch_bounds__(TcShape<WS>::THREADS, 1) xcorr_tc_kernel(const
     constexpr int LDF = WS + 1;     // plane row stride (peak stage)
     constexpr uint32_t G_BYTES = S::G_BYTES, A_BYTES = S::A_BYTES;
     constexpr uint32_t TCOLS = S::TCOLS, TALLOC = S::TCOLS * S::NG;
-    // operand scales (powers of two): pass B 1/WS, cross spectrum 1/(2 WS^2), pass D 1/(2 WS);
-    // the plane is |out| * (2 WS * 2 WS^2 * WS^2) / N = |out| * 4 WS^3, one exact multiply
-    constexpr float sB = 1.0f / (float)WS, sC = 1.0f / (float)(2 * WS * WS), sD = 1.0f / (float)(2 * WS);
-    constexpr float out_scale = (float)(4 * WS * WS * WS);
+    // operand scales (powers of two, exact): FP16 operands take pass B's by 1/WS, the cross
+    // spectrum's by 1/(2 WS^2) and pass D's by 1/(2 WS), which keep every value of any 8-bit
+    // window pair below 65504; BF16 has FP32's exponent range and keeps only the cross
+    // spectrum's, folded into its constant factors.  The plane is |out| / (sB^2 sC sD N), one
+    // exact multiply (4 WS^3 with FP16 operands, 2 with BF16).
+    constexpr float sB = F16 ? 1.0f / (float)WS : 1.0f, sC = 1.0f / (float)(2 * WS * WS);
+    constexpr float sD = F16 ? 1.0f / (float)(2 * WS) : 1.0f;
+    constexpr float out_scale = 1.0f / (sB * sB * sC * sD * (float)(WS * WS));
     static_assert(TALLOC == 32 || TALLOC == 64 || TALLOC == 128 || TALLOC == 256 || TALLOC == 512, "TMEM alloc");
     static_assert((size_t)NWIN * WS * LDF * 4 <= 2 * A_BYTES, "planes fit in the A buffers");
 
@@ -416,21 +454,19 @@ __global__ void __launch_bounds__(TcShape<WS>::THREADS, 1) xcorr_tc_kernel(const
 #pragma unroll
                 for (int i = 0; i < WS; ++i) v1[i] = v2[i] = 0.f;
             }
-            bool nz1 = false, nz2 = false;
-#pragma unroll
-            for (int i = 0; i < WS; ++i) {
-                nz1 |= v1[i] != 0.f;
-                nz2 |= v2[i] != 0.f;
-            }
-            const uint32_t b1 = __ballot_sync(0xffffffffu, nz1), b2 = __ballot_sync(0xffffffffu, nz2);
+            const uint32_t b1 = __ballot_sync(0xffffffffu, any_nonzero<WS>(v1));
+            const uint32_t b2 = __ballot_sync(0xffffffffu, any_nonzero<WS>(v2));
             if (lane == 0) {
                 s_nz1[wg][wq] = b1;
                 s_nz2[wg][wq] = b2;
             }
 #pragma unroll
             for (int c = 0; c < WS / 8; ++c) {
-                store8<NPROD, F16>(a_hi, a_lo, tc::off_kmajor(lt, 8 * c, 128), v1 + 8 * c);
-                store8<NPROD, F16>(a_hi, a_lo, tc::off_kmajor(lt, WS + 8 * c, 128), v2 + 8 * c);
+                // frame 1 (and frame 2 when undeformed) holds integers, exact in the operand
+                // type: their lo part is zero and the MMAs skip it (LO_FROM)
+                store8_exact<F16>(a_hi, tc::off_kmajor(lt, 8 * c, 128), v1 + 8 * c);
+                if constexpr (DEF) store8<NPROD, F16>(a_hi, a_lo, tc::off_kmajor(lt, WS + 8 * c, 128), v2 + 8 * c);
+                else store8_exact<F16>(a_hi, tc::off_kmajor(lt, WS + 8 * c, 128), v2 + 8 * c);
             }
         }
         if (!sync_issue(ok_rows)) {
@@ -466,8 +502,8 @@ __global__ void __launch_bounds__(TcShape<WS>::THREADS, 1) xcorr_tc_kernel(const
                         br[i] = zr[col_at<WS>(8 * c + i)];
                         bi[i] = zi[col_at<WS>(8 * c + i)];
                     }
-                    store8s<NPROD, F16>(a_hi, a_lo, tc::off_mnmajor(wl * WS + 8 * c, r, KK), br, sB);
-                    store8s<NPROD, F16>(a_hi, a_lo, tc::off_mnmajor(wl * WS + 8 * c, WS + r, KK), bi, sB);
+                    store8s<NPROD, F16, F16>(a_hi, a_lo, tc::off_mnmajor(wl * WS + 8 * c, r, KK), br, sB);
+                    store8s<NPROD, F16, F16>(a_hi, a_lo, tc::off_mnmajor(wl * WS + 8 * c, WS + r, KK), bi, sB);
                 }
             }
             if (!sync_issue(ok)) {
@@ -497,11 +533,12 @@ __global__ void __launch_bounds__(TcShape<WS>::THREADS, 1) xcorr_tc_kernel(const
                         const int ky = 8 * c + i, km = (WS - ky) % WS;
                         const float pr = __shfl_sync(0xffffffffu, zr[km], partner);
                         const float pi = __shfl_sync(0xffffffffu, zi[km], partner);
-                        cr[i] = dead ? 0.f : 0.5f * (zr[ky] * pi + zi[ky] * pr);
-                        ci[i] = dead ? 0.f : 0.25f * ((pr * pr + pi * pi) - (zr[ky] * zr[ky] + zi[ky] * zi[ky]));
+                        // scaled by sC, folded into the exact constant factors
+                        cr[i] = dead ? 0.f : (0.5f * sC) * (zr[ky] * pi + zi[ky] * pr);
+                        ci[i] = dead ? 0.f : (0.25f * sC) * ((pr * pr + pi * pi) - (zr[ky] * zr[ky] + zi[ky] * zi[ky]));
                     }
-                    store8s<NPROD, F16>(a_hi, a_lo, tc::off_kmajor(lt, 8 * c, 128), cr, sC);
-                    store8s<NPROD, F16>(a_hi, a_lo, tc::off_kmajor(lt, WS + 8 * c, 128), ci, sC);
+                    store8<NPROD, F16>(a_hi, a_lo, tc::off_kmajor(lt, 8 * c, 128), cr);
+                    store8<NPROD, F16>(a_hi, a_lo, tc::off_kmajor(lt, WS + 8 * c, 128), ci);
                 }
             }
             if (!sync_issue(ok)) {
@@ -524,8 +561,8 @@ __global__ void __launch_bounds__(TcShape<WS>::THREADS, 1) xcorr_tc_kernel(const
                 tc::tmem_wait_ld();
 #pragma unroll
                 for (int c = 0; c < WS / 8; ++c) {
-                    store8s<NPROD, F16>(a_hi, a_lo, tc::off_mnmajor(wl * WS + 8 * c, kx, KK), tr + 8 * c, sD);
-                    store8s<NPROD, F16>(a_hi, a_lo, tc::off_mnmajor(wl * WS + 8 * c, WS + kx, KK), ti + 8 * c, sD);
+                    store8s<NPROD, F16, F16>(a_hi, a_lo, tc::off_mnmajor(wl * WS + 8 * c, kx, KK), tr + 8 * c, sD);
+                    store8s<NPROD, F16, F16>(a_hi, a_lo, tc::off_mnmajor(wl * WS + 8 * c, WS + kx, KK), ti + 8 * c, sD);
                 }
             }
             if (!sync_issue(ok)) {

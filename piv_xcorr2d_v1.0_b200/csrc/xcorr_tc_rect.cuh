@@ -153,10 +153,16 @@ __global__ void __launch_bounds__(TcRectShape<WX, WY>::THREADS, 1) xcorr_tc_rect
     constexpr int LDF = WX + 1;  // plane row stride (peak stage)
     constexpr uint32_t GX_BYTES = S::GX_BYTES, GY_BYTES = S::GY_BYTES, A_BYTES = S::A_BYTES;
     constexpr uint32_t TCOLS = S::TCOLS, TALLOC = 512;
-    // operand scales (powers of two): pass B 1/PX, cross spectrum 1/(2 PY^2), pass D 1/(2 PY)
+    // operand scales (powers of two, exact): FP16 operands take pass B's by 1/PX, the cross
+    // spectrum's by 1/(2 PY^2) and pass D's by 1/(2 PY); BF16 (FP32's exponent range) keeps only
+    // the cross spectrum's, folded into its constant factors
     constexpr int PX = pow2_at_least(WX), PY = pow2_at_least(WY);
-    constexpr float sB = 1.0f / (float)PX, sC = 1.0f / (float)(2 * PY * PY), sD = 1.0f / (float)(2 * PY);
-    constexpr float unscale = (float)PX * (float)PX * (float)(2 * PY * PY) * (float)(2 * PY);
+    constexpr float sB = F16 ? 1.0f / (float)PX : 1.0f, sC = 1.0f / (float)(2 * PY * PY);
+    constexpr float sD = F16 ? 1.0f / (float)(2 * PY) : 1.0f;
+    constexpr float unscale = 1.0f / (sB * sB * sC * sD);
+    // pass A's lo products start at this K step (frame 1, and frame 2 when undeformed, hold
+    // integers exact in the operand type)
+    constexpr int LOF = DEF ? WX / 16 : KX / 16;
     constexpr float inv_n = 1.0f / (float)(WX * WY);
     static_assert(2 * WY * LDF * 4 + 2 * sizeof(PeakPart[2]) <= 2 * A_BYTES, "planes and peak scratch fit");
 
@@ -239,27 +245,25 @@ __global__ void __launch_bounds__(TcRectShape<WX, WY>::THREADS, 1) xcorr_tc_rect
 #pragma unroll
                 for (int i = 0; i < WX; ++i) v1[i] = v2[i] = 0.f;
             }
-            bool nz1 = false, nz2 = false;
-#pragma unroll
-            for (int i = 0; i < WX; ++i) {
-                nz1 |= v1[i] != 0.f;
-                nz2 |= v2[i] != 0.f;
-            }
-            const uint32_t b1 = __ballot_sync(0xffffffffu, nz1), b2 = __ballot_sync(0xffffffffu, nz2);
+            const uint32_t b1 = __ballot_sync(0xffffffffu, any_nonzero<WX>(v1));
+            const uint32_t b2 = __ballot_sync(0xffffffffu, any_nonzero<WX>(v2));
             if (lane == 0) {
                 s_nz1[wg][wq] = b1;
                 s_nz2[wg][wq] = b2;
             }
 #pragma unroll
             for (int c = 0; c < WX / 8; ++c) {
-                store8<NPROD, F16>(a_hi, a_lo, tc::off_kmajor(lt, 8 * c, 128), v1 + 8 * c);
-                store8<NPROD, F16>(a_hi, a_lo, tc::off_kmajor(lt, WX + 8 * c, 128), v2 + 8 * c);
+                // integer columns below the lo products' first K step: the hi part only
+                if (8 * c + 8 <= 16 * LOF) store8_exact<F16>(a_hi, tc::off_kmajor(lt, 8 * c, 128), v1 + 8 * c);
+                else store8<NPROD, F16>(a_hi, a_lo, tc::off_kmajor(lt, 8 * c, 128), v1 + 8 * c);
+                if (WX + 8 * c + 8 <= 16 * LOF) store8_exact<F16>(a_hi, tc::off_kmajor(lt, WX + 8 * c, 128), v2 + 8 * c);
+                else store8<NPROD, F16>(a_hi, a_lo, tc::off_kmajor(lt, WX + 8 * c, 128), v2 + 8 * c);
             }
         }
         if (!sync_issue(true)) break;
         if (lt == 0) {
             // frame 1 is integer-valued (exact in the 16-bit formats); frame 2 only when deformed
-            issue_pass<KX, KX, false, true, NPROD, DEF ? WX / 16 : KX / 16, F16>(tmem, sa_hi, sa_lo, sgx_hi, sgx_lo);
+            issue_pass<KX, KX, false, true, NPROD, LOF, F16>(tmem, sa_hi, sa_lo, sgx_hi, sgx_lo);
             tc::mma_commit(mb);
         }
         // windows with an all-zero frame: spectrum and plane 0 (the reference's exact zeros)
@@ -284,8 +288,8 @@ __global__ void __launch_bounds__(TcRectShape<WX, WY>::THREADS, 1) xcorr_tc_rect
                             br[i] = zr[col];
                             bi[i] = zi[col];
                         }
-                        store8s<NPROD, F16>(a_hi, a_lo, tc::off_mnmajor(wlA * WX + 8 * c, y, KY), br, sB);
-                        store8s<NPROD, F16>(a_hi, a_lo, tc::off_mnmajor(wlA * WX + 8 * c, WY + y, KY), bi, sB);
+                        store8s<NPROD, F16, F16>(a_hi, a_lo, tc::off_mnmajor(wlA * WX + 8 * c, y, KY), br, sB);
+                        store8s<NPROD, F16, F16>(a_hi, a_lo, tc::off_mnmajor(wlA * WX + 8 * c, WY + y, KY), bi, sB);
                     }
                 }
             }
@@ -315,12 +319,13 @@ __global__ void __launch_bounds__(TcRectShape<WX, WY>::THREADS, 1) xcorr_tc_rect
                         const int ky = 8 * c + i, km = (WY - ky) % WY;
                         const float pr = __shfl_sync(0xffffffffu, zr[km], partner);
                         const float pi = __shfl_sync(0xffffffffu, zi[km], partner);
-                        cr[i] = deadB ? 0.f : 0.5f * (zr[ky] * pi + zi[ky] * pr);
-                        ci[i] = deadB ? 0.f : 0.25f * ((pr * pr + pi * pi) - (zr[ky] * zr[ky] + zi[ky] * zi[ky]));
+                        // scaled by sC, folded into the exact constant factors
+                        cr[i] = deadB ? 0.f : (0.5f * sC) * (zr[ky] * pi + zi[ky] * pr);
+                        ci[i] = deadB ? 0.f : (0.25f * sC) * ((pr * pr + pi * pi) - (zr[ky] * zr[ky] + zi[ky] * zi[ky]));
                     }
                     if (rowB) {
-                        store8s<NPROD, F16>(a_hi, a_lo, tc::off_kmajor(lt, 8 * c, 128), cr, sC);
-                        store8s<NPROD, F16>(a_hi, a_lo, tc::off_kmajor(lt, WY + 8 * c, 128), ci, sC);
+                        store8<NPROD, F16>(a_hi, a_lo, tc::off_kmajor(lt, 8 * c, 128), cr);
+                        store8<NPROD, F16>(a_hi, a_lo, tc::off_kmajor(lt, WY + 8 * c, 128), ci);
                     }
                 }
             }
@@ -345,8 +350,8 @@ __global__ void __launch_bounds__(TcRectShape<WX, WY>::THREADS, 1) xcorr_tc_rect
                 if (rowB) {
 #pragma unroll
                     for (int c = 0; c < WY / 8; ++c) {
-                        store8s<NPROD, F16>(a_hi, a_lo, tc::off_mnmajor(wlB * WY + 8 * c, kx, KX), tr + 8 * c, sD);
-                        store8s<NPROD, F16>(a_hi, a_lo, tc::off_mnmajor(wlB * WY + 8 * c, WX + kx, KX), ti + 8 * c, sD);
+                        store8s<NPROD, F16, F16>(a_hi, a_lo, tc::off_mnmajor(wlB * WY + 8 * c, kx, KX), tr + 8 * c, sD);
+                        store8s<NPROD, F16, F16>(a_hi, a_lo, tc::off_mnmajor(wlB * WY + 8 * c, WX + kx, KX), ti + 8 * c, sD);
                     }
                 }
             }
