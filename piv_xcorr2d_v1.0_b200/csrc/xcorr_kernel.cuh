@@ -29,7 +29,7 @@
 //   P5  warp per window (two warps for windows taller than 32 rows when the CTA has
 //       them): 4-neighbour local maxima inside the search region,
 //       count, register top-K (value desc, then lower index), 3-point Gaussian fit
-//       with an FP64 log-ratio denominator, predictor, limits, NaN/Inf removal.
+//       with an accurate log-ratio denominator, predictor, limits, NaN/Inf removal.
 #pragma once
 #include <cfloat>
 #include <climits>
@@ -226,6 +226,21 @@ __device__ __forceinline__ void peak_select(int Nps, int lane, float (&tv)[K], i
     }
 }
 
+// ln(fm fp / c^2), the Gaussian fit's denominator, which cancels near flat peaks (the
+// reference's ln fm + ln fp - 2 ln c in FP32 loses most of its bits there).  fm fp - c^2 is
+// formed exactly, up to one rounding, from the two products and their FMA residuals, divided
+// by c^2 and passed to log1pf: about 2 ulp of the true value, as FP64 would give after the
+// final rounding to FP32, without FP64 arithmetic.  Products below 2^-100, where they would
+// lose bits to underflow, take the FP64 form.
+__device__ __forceinline__ float fit_denominator(float fm, float fp, float c)
+{
+    const float p = fm * fp, q = c * c;
+    if (!(p >= 7.8886091e-31f && q >= 7.8886091e-31f))  // 2^-100; also zeros and NaN
+        return (float)log(((double)fm * (double)fp) / ((double)c * (double)c));
+    const float ep = fmaf(fm, fp, -p), eq = fmaf(c, c, -q);
+    return log1pf(((p - q) + (ep - eq)) / q);
+}
+
 // Sub-pixel fit of the candidates held by lanes < Nps, limits, NaN/Inf removal and the
 // stores of the window's outputs; cnt is the window's count of maxima.  Called by whole
 // warps (the fits' x and y halves run on separate lanes and meet by shuffle).
@@ -250,12 +265,10 @@ __device__ __forceinline__ void peak_fit_store(const XcorrArgs &a, const float *
             const float *pc = P + j * LDF + i;
             const int step = comp ? LDF : 1;
             const float f0 = pc[-step], f2 = pc[step];
-            const double dv = (double)cv * (double)cv;
-            // numerator ln f- - ln f+ in FP32 as the reference; the cancelling
-            // denominator ln(f- f+ / f0^2) in FP64
+            // numerator ln f- - ln f+ in FP32 as the reference; the cancelling denominator
+            // ln(f- f+ / f0^2) accurately (fit_denominator)
             const float nn = logf(f0) - logf(f2);
-            const double den = log(((double)f0 * (double)f2) / dv);
-            sh = (float)((double)nn / den / 2.0);
+            sh = nn / fit_denominator(f0, f2, cv) * 0.5f;
             inner = true;
         }
     }
