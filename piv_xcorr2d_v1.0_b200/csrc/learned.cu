@@ -483,10 +483,38 @@ __global__ void __launch_bounds__(512, 1) conv_tc_kernel(const ConvFwd c, int *s
     // K-major A: byte (k/8)*2048 + m*16 + (k%8)*2 with m = px_id; this thread's channels
     // k = 4*quarter .. + 3 are 8 bytes at (quarter/2)*2048 + m*16 + (quarter%2)*8
     const uint32_t a_off = (uint32_t)(quarter >> 1) * 2048u + (uint32_t)px_id * 16u + (uint32_t)(quarter & 1) * 8u;
+    // the 9 taps' weights of a channel block, (tap, g = co/8, k) at byte (co/8)*256 + k*16 of
+    // the tap's B operand: loaded into registers one block ahead (their global latency
+    // overlaps the operand build of the block before), stored once the buffer is free
+    constexpr int WPT = (9 * 2 * N + 511) / 512;  // 16-byte chunks per thread
+    uint4 wreg[WPT];
+    auto load_w = [&](int b) {
+#pragma unroll
+        for (int i = 0; i < WPT; ++i) {
+            const int e = tid + 512 * i;
+            wreg[i] = make_uint4(0u, 0u, 0u, 0u);
+            if (e < 9 * 2 * N) {
+                const int tap = e / (2 * N), r = e - tap * (2 * N), g = r / kTcCB, k = r - g * kTcCB;
+                const int cc = b * kTcCB + k;
+                if (cc < cin) wreg[i] = __ldg(reinterpret_cast<const uint4 *>(c.w + ((size_t)cc * 9 + tap) * c.cout) + g);
+            }
+        }
+    };
+    auto store_w = [&](int bb) {
+#pragma unroll
+        for (int i = 0; i < WPT; ++i) {
+            const int e = tid + 512 * i;
+            if (e < 9 * 2 * N) {
+                const int tap = e / (2 * N), r = e - tap * (2 * N), g = r / kTcCB, k = r - g * kTcCB;
+                reinterpret_cast<uint4 *>(S.b[bb][tap])[g * kTcCB + k] = wreg[i];
+            }
+        }
+    };
+    load_w(0);
     bool ok = true;
     int blk = 0;
     for (; blk < nblk; ++blk) {
-        const int bb = blk & 1, cb0 = blk * kTcCB;
+        const int bb = blk & 1;
         // the next block's patch streams in while this one is built (its buffer was last
         // read by block blk - 1's operand build, finished before that block's MMA barrier)
         if (blk + 1 < nblk) {
@@ -507,13 +535,8 @@ __global__ void __launch_bounds__(512, 1) conv_tc_kernel(const ConvFwd c, int *s
             __syncthreads();  // every thread's patch copies have landed
         }
         float(*patch)[kTcPY][kTcPX] = S.patch[bb];
-        // the weights of the block's 9 taps: chunk (tap, g = co/8, k) at byte (co/8)*256 + k*16
-        for (int e = tid; e < 9 * 2 * N; e += 512) {
-            const int tap = e / (2 * N), r = e - tap * (2 * N), g = r / kTcCB, k = r - g * kTcCB, cc = cb0 + k;
-            uint4 w = make_uint4(0u, 0u, 0u, 0u);
-            if (cc < cin) w = __ldg(reinterpret_cast<const uint4 *>(c.w + ((size_t)cc * 9 + tap) * c.cout) + g);
-            reinterpret_cast<uint4 *>(S.b[bb][tap])[g * kTcCB + k] = w;
-        }
+        store_w(bb);
+        if (blk + 1 < nblk) load_w(blk + 1);
 #pragma unroll 1
         for (int tap = 0; tap < 9; ++tap) {
             const int ky = tap / 3, kx = tap - ky * 3;
