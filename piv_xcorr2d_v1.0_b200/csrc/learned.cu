@@ -286,7 +286,7 @@ constexpr size_t conv_fwd_smem()
 }
 
 template <int COT>
-__global__ void __launch_bounds__(256) conv_fwd_kernel(const ConvFwd c)
+__global__ void __launch_bounds__(256, 2) conv_fwd_kernel(const ConvFwd c)
 {
     constexpr int NW = kConvWarps;
     extern __shared__ __align__(16) float csm[];
@@ -304,51 +304,100 @@ __global__ void __launch_bounds__(256) conv_fwd_kernel(const ConvFwd c)
     float acc[COT];
 #pragma unroll
     for (int k = 0; k < COT; ++k) acc[k] = 0.f;
-#pragma unroll 1
-    for (int ci = split * 2 * NW + warp; ci < cin; ci += 2 * NW * c.splits) {
-        const int cj = ci + NW;
-        const bool two = cj < cin;
-        // both channels' weights: for each tap a contiguous run of COT output channels
-        if constexpr (COT % 8 == 0) {
-            constexpr int Q = COT / 8;  // 16-byte chunks per run
-            for (int e = lane; e < 2 * 9 * Q; e += 32) {
-                const int ch = e / (9 * Q), r = e - ch * (9 * Q), tap = r / Q, q = r - tap * Q;
-                const int cc = ch ? cj : ci;
-                uint4 u = make_uint4(0u, 0u, 0u, 0u);
-                if (ch == 0 || two)
-                    u = __ldg(reinterpret_cast<const uint4 *>(c.w + ((size_t)cc * 9 + tap) * c.cout + co0) + q);
-                const __nv_bfloat162 *h = reinterpret_cast<const __nv_bfloat162 *>(&u);
-                const float2 f0 = __bfloat1622float2(h[0]), f1 = __bfloat1622float2(h[1]);
-                const float2 f2 = __bfloat1622float2(h[2]), f3 = __bfloat1622float2(h[3]);
-                float4 *dst = reinterpret_cast<float4 *>(&wsm[warp][ch][tap][8 * q]);  // 16-byte stores
-                dst[0] = make_float4(f0.x, f0.y, f1.x, f1.y);
-                dst[1] = make_float4(f2.x, f2.y, f3.x, f3.y);
+    const int step = 2 * NW * c.splits;
+    if constexpr (COT % 8 == 0) {
+        // Each iteration's weights (raw BF16 chunks) and input taps are loaded into registers
+        // one iteration ahead, so that their global latency overlaps the FMAs before them.
+        constexpr int Q = COT / 8;                         // 16-byte chunks per tap run
+        constexpr int WPL = (2 * 9 * Q + 31) / 32;         // chunks per lane
+        uint4 wn[WPL];
+        float xn0[9], xn1[9];
+        auto prefetch = [&](int ci) {
+            const int cj = ci + NW;
+            const bool two = cj < cin;
+#pragma unroll
+            for (int i = 0; i < WPL; ++i) {
+                const int e = lane + 32 * i;
+                wn[i] = make_uint4(0u, 0u, 0u, 0u);
+                if (e < 2 * 9 * Q) {
+                    const int ch = e / (9 * Q), r = e - ch * (9 * Q), tap = r / Q, q = r - tap * Q;
+                    if (ch == 0 || two)
+                        wn[i] = __ldg(reinterpret_cast<const uint4 *>(c.w + ((size_t)(ch ? cj : ci) * 9 + tap) * c.cout + co0) + q);
+                }
             }
-        } else {
+            conv_gather(c.in, n, ci, oa, ob, xn0);
+            if (two) {
+                conv_gather(c.in, n, cj, oa, ob, xn1);
+            } else {
+#pragma unroll
+                for (int t = 0; t < 9; ++t) xn1[t] = 0.f;
+            }
+        };
+        int ci = split * 2 * NW + warp;
+        if (ci < cin) prefetch(ci);
+#pragma unroll 1
+        for (; ci < cin; ci += step) {
+            // this iteration's weights into the warp's slices (FMAs read broadcasts)
+#pragma unroll
+            for (int i = 0; i < WPL; ++i) {
+                const int e = lane + 32 * i;
+                if (e < 2 * 9 * Q) {
+                    const int ch = e / (9 * Q), r = e - ch * (9 * Q), tap = r / Q, q = r - tap * Q;
+                    const __nv_bfloat162 *h = reinterpret_cast<const __nv_bfloat162 *>(&wn[i]);
+                    const float2 f0 = __bfloat1622float2(h[0]), f1 = __bfloat1622float2(h[1]);
+                    const float2 f2 = __bfloat1622float2(h[2]), f3 = __bfloat1622float2(h[3]);
+                    float4 *dst = reinterpret_cast<float4 *>(&wsm[warp][ch][tap][8 * q]);  // 16-byte stores
+                    dst[0] = make_float4(f0.x, f0.y, f1.x, f1.y);
+                    dst[1] = make_float4(f2.x, f2.y, f3.x, f3.y);
+                }
+            }
+            float x0[9], x1[9];
+#pragma unroll
+            for (int t = 0; t < 9; ++t) {
+                x0[t] = xn0[t];
+                x1[t] = xn1[t];
+            }
+            __syncwarp();
+            if (ci + step < cin) prefetch(ci + step);
+#pragma unroll
+            for (int t = 0; t < 9; ++t)
+#pragma unroll
+                for (int k = 0; k < COT; ++k) acc[k] = fmaf(wsm[warp][0][t][k], x0[t], acc[k]);
+#pragma unroll
+            for (int t = 0; t < 9; ++t)
+#pragma unroll
+                for (int k = 0; k < COT; ++k) acc[k] = fmaf(wsm[warp][1][t][k], x1[t], acc[k]);
+            __syncwarp();
+        }
+    } else {
+#pragma unroll 1
+        for (int ci = split * 2 * NW + warp; ci < cin; ci += step) {
+            const int cj = ci + NW;
+            const bool two = cj < cin;
             for (int e = lane; e < 2 * 9 * COT; e += 32) {
                 const int ch = e / (9 * COT), r = e - ch * (9 * COT), tap = r / COT, co = r - tap * COT;
                 const int cc = ch ? cj : ci;
                 const bool ok = co0 + co < c.cout && (ch == 0 || two);
                 wsm[warp][ch][tap][co] = ok ? __bfloat162float(c.w[((size_t)cc * 9 + tap) * c.cout + co0 + co]) : 0.f;
             }
+            __syncwarp();
+            float x0[9], x1[9];
+            conv_gather(c.in, n, ci, oa, ob, x0);
+            if (two) conv_gather(c.in, n, cj, oa, ob, x1);
+            else {
+#pragma unroll
+                for (int t = 0; t < 9; ++t) x1[t] = 0.f;
+            }
+#pragma unroll
+            for (int t = 0; t < 9; ++t)
+#pragma unroll
+                for (int k = 0; k < COT; ++k) acc[k] = fmaf(wsm[warp][0][t][k], x0[t], acc[k]);
+#pragma unroll
+            for (int t = 0; t < 9; ++t)
+#pragma unroll
+                for (int k = 0; k < COT; ++k) acc[k] = fmaf(wsm[warp][1][t][k], x1[t], acc[k]);
+            __syncwarp();
         }
-        __syncwarp();
-        float x0[9], x1[9];
-        conv_gather(c.in, n, ci, oa, ob, x0);
-        if (two) conv_gather(c.in, n, cj, oa, ob, x1);
-        else {
-#pragma unroll
-            for (int t = 0; t < 9; ++t) x1[t] = 0.f;
-        }
-#pragma unroll
-        for (int t = 0; t < 9; ++t)
-#pragma unroll
-            for (int k = 0; k < COT; ++k) acc[k] = fmaf(wsm[warp][0][t][k], x0[t], acc[k]);
-#pragma unroll
-        for (int t = 0; t < 9; ++t)
-#pragma unroll
-            for (int k = 0; k < COT; ++k) acc[k] = fmaf(wsm[warp][1][t][k], x1[t], acc[k]);
-        __syncwarp();
     }
     __syncthreads();  // every warp is done with its weight slices: the reduction reuses them
 #pragma unroll
