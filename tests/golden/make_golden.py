@@ -29,13 +29,13 @@ from oracle import ref as R  # noqa: E402
 
 # name -> (synthetic-input kwargs, engine parameter overrides)
 CASES = {
-    # 1024^2, uniform (3.3, -1.7), single 32x32 grid at 50 %, 1 pass, top-4, pct 0.25, threshold 2
+    # the 1024^2 single-grid case: uniform (3.3, -1.7), 32x32 windows at 50 %, 1 pass, top-4, pct 0.25, threshold 2
     "c0": (dict(Nx=1024, Ny=1024, ppp=0.05, field=P.PIV_FIELD_UNIFORM, a=3.3, b=-1.7, seed=1),
            dict(Nx=1024, Ny=1024, ws_x1=32, ws_y1=32, spacing_x1=16, spacing_y1=16, Npass1=1,
                 ws_x2=32, ws_y2=32, spacing_x2=16, spacing_y2=16, Npass2=0,
                 max_dispx_win_percent1=0.25, max_dispy_win_percent1=0.25, max_dispx_win_percent2=0.25,
                 max_dispy_win_percent2=0.25, insert_threshold_p1=2.0, insert_threshold_p2=2.0)),
-    # a small configs[1]: Lamb-Oseen vortex + shear, MHE (40 px, 0.91, non-divisible crop), 64->32 multigrid
+    # a small form of the 6600x4400 multigrid case: Lamb-Oseen vortex + shear, MHE (40 px, 0.91, non-divisible crop), 64->32
     "multigrid": (dict(Nx=520, Ny=392, ppp=0.04, field=P.PIV_FIELD_VORTEX, a=6.0, b=120.0, c=0.002, seed=2),
                   dict(Nx=520, Ny=392, if_mhe=1, mhe_ws=40, mhe_thresh=0.91, Npass1=2, Npass2=3,
                        insert_threshold_p1=2.0, insert_threshold_p2=2.0, max_dispx_win_percent1=0.25,
