@@ -64,6 +64,11 @@ cudaError_t launch_shape(const XcorrArgs &a, bool deformed, int K, cudaStream_t 
 #define PIV_X(WX, WY, B, NT) extern template cudaError_t launch_shape<WX, WY, B, NT>(const XcorrArgs &, bool, int, cudaStream_t);
 PIV_XCORR_VARIANTS(PIV_X)
 #undef PIV_X
+// the 2x2-block form (four windows of two window rows per CTA), listed after the shape's
+// row-major variants
+template <int WSX, int WSY, int NT>
+cudaError_t launch_shape_block(const XcorrArgs &a, bool deformed, int K, cudaStream_t s);
+extern template cudaError_t launch_shape_block<32, 32, 128>(const XcorrArgs &, bool, int, cudaStream_t);
 
 // Variants of the persistent batch launch (two per shape; the batch autotuner picks one
 // per shape group).
@@ -109,6 +114,7 @@ const Variant kVariants[] = {
 #define PIV_X(WX, WY, B, NT) {WX, WY, B, NT, &launch_shape<WX, WY, B, NT>},
     PIV_XCORR_VARIANTS(PIV_X)
 #undef PIV_X
+    {32, 32, 4, 128, &launch_shape_block<32, 32, 128>},
 };
 constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
 

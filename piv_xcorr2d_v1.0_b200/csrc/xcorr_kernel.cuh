@@ -411,6 +411,18 @@ constexpr int xcorr_min_ctas()
 template <int WSX, int WSY, int B, int NT, int K, bool DEF>
 __global__ void __launch_bounds__(NT, (xcorr_min_ctas<WSX, WSY, B, NT>())) xcorr_peak_kernel(const XcorrArgs a)
 {
+    constexpr int VB = 1;
+    const unsigned blk = blockIdx.x;
+#include "xcorr_body.inc"
+}
+
+// 2x2-block form: a CTA takes two horizontally adjacent window pairs in two consecutive window
+// rows, whose overlapping pixel rows are gathered and row-transformed once (at 50 % overlap 3/4
+// of the row transforms of the row-major form).  Same arithmetic per window, so the same bits.
+template <int WSX, int WSY, int NT, int K, bool DEF>
+__global__ void __launch_bounds__(NT, (xcorr_min_ctas<WSX, WSY, 4, NT>())) xcorr_block_kernel(const XcorrArgs a)
+{
+    constexpr int B = 4, VB = 2;
     const unsigned blk = blockIdx.x;
 #include "xcorr_body.inc"
 }
@@ -435,6 +447,7 @@ __global__ void __launch_bounds__(NT, (xcorr_min_ctas<WSX, WSY, B, NT>())) xcorr
     }
     const XcorrArgs &a = b.pairs[lo];
     const unsigned blk = it - b.first[lo];
+    constexpr int VB = 1;
 #include "xcorr_body.inc"
 }
 
@@ -461,6 +474,35 @@ cudaError_t launch_shape(const XcorrArgs &a, bool deformed, int K, cudaStream_t 
     } else {
         if (deformed) go(xcorr_peak_kernel<WSX, WSY, B, NT, 8, true>);
         else go(xcorr_peak_kernel<WSX, WSY, B, NT, 8, false>);
+    }
+    return e;
+}
+
+// Launch of the 2x2-block form (four windows per CTA): the blocks of the launch's window rows
+// (rounded out to whole block rows; windows outside [w_first, w_end) are computed, not
+// written).  An odd row of windows has no whole pairs of columns: the row-major form then.
+template <int WSX, int WSY, int NT>
+cudaError_t launch_shape_block(const XcorrArgs &a, bool deformed, int K, cudaStream_t s)
+{
+    if (a.w_end <= a.w_first) return cudaSuccess;
+    const int nx = a.g.Nx_vec;
+    if (nx % 2) return launch_shape<WSX, WSY, 4, NT>(a, deformed, K, s);
+    const int by0 = (a.w_first / nx) >> 1, by1 = ((a.w_end - 1) / nx) >> 1;
+    const size_t smem = (size_t)4 * WSY * (WSX + 1) * sizeof(float2);
+    dim3 grid((unsigned)((nx >> 1) * (by1 - by0 + 1)));
+    cudaError_t e = cudaSuccess;
+    auto go = [&](auto kern) {
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return;
+        kern<<<grid, NT, smem, s>>>(a);
+        e = cudaGetLastError();
+    };
+    if (K <= 4) {
+        if (deformed) go(xcorr_block_kernel<WSX, WSY, NT, 4, true>);
+        else go(xcorr_block_kernel<WSX, WSY, NT, 4, false>);
+    } else {
+        if (deformed) go(xcorr_block_kernel<WSX, WSY, NT, 8, true>);
+        else go(xcorr_block_kernel<WSX, WSY, NT, 8, false>);
     }
     return e;
 }

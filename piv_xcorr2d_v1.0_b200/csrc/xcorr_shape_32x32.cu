@@ -8,6 +8,7 @@ template cudaError_t launch_shape<32, 32, 4, 128>(const XcorrArgs &, bool, int, 
 template cudaError_t launch_shape<32, 32, 2, 64>(const XcorrArgs &, bool, int, cudaStream_t);
 template cudaError_t launch_shape<32, 32, 8, 256>(const XcorrArgs &, bool, int, cudaStream_t);
 template cudaError_t launch_shape<32, 32, 4, 64>(const XcorrArgs &, bool, int, cudaStream_t);
+template cudaError_t launch_shape_block<32, 32, 128>(const XcorrArgs &, bool, int, cudaStream_t);
 template cudaError_t launch_shape_batch<32, 32, 4, 128>(const XcorrBatch &, bool, int, cudaStream_t);
 template cudaError_t launch_shape_batch<32, 32, 8, 128>(const XcorrBatch &, bool, int, cudaStream_t);
 }

@@ -179,3 +179,34 @@ def test_batch_runs_a_members_tensor_core_path(cuda):
                     assert np.array_equal(u, v), (i, s)
     # and its result is the tensor-core one, not the SIMT one
     assert not all(np.array_equal(u, v) for u, v in zip(got[-1][2][2], simt[0][2]))
+
+
+BLOCK_32 = 5  # index of the 2x2-block form among the 32x32 variants (after the row-major ones)
+
+
+@pytest.mark.parametrize("Nx,Ny,sp,nsec", [(432, 344, 8, 1), (432, 344, 8, 7), (448, 352, 32, 1), (448, 352, 32, 3),
+                                           (432, 344, 16, 1), (416, 328, 16, 5)],
+                         ids=["75pc-rows-odd", "75pc-7-sections", "no-overlap", "no-overlap-3-sections",
+                              "odd-row-fallback", "50pc-5-sections"])
+def test_block_form_gives_the_same_bits(cuda, monkeypatch, Nx, Ny, sp, nsec):
+    """The 2x2-block form (two window rows per CTA sharing their overlapping pixel rows)
+    against the row-major 4 x 128 form: window grids with an odd number of rows (a partial
+    last block row), 75 %, 50 % and no overlap, sections starting inside a block row, an odd
+    row of windows (the form falls back to the row-major launch), and a plane dump starting
+    at an odd window."""
+    f1, f2 = _frames(Nx, Ny, seed=900 + sp + nsec)
+    p = P.default_params(Nx=Nx, Ny=Ny, ws_x1=32, ws_y1=32, spacing_x1=sp, spacing_y1=sp, Npass1=2, Npass2=0,
+                         Nsec_cc=nsec, insert_threshold_p1=2.0, max_dispx_win_percent1=0.25,
+                         max_dispy_win_percent1=0.25)
+    res = []
+    for v in (1, BLOCK_32):
+        monkeypatch.setenv("PIV_XCORR_VARIANT", f"{v},0")
+        with P.Engine(p) as e:
+            e.set_images(f1, f2)
+            e.run_pair()
+            e.synchronize()
+            assert e.xcorr_config(0)[:2] == (4, 128)
+            nt = e.geom["Nt_vec"][0]
+            res.append((_outputs(e, [0]), e.cc_planes(0, 37, min(300, nt - 40))))
+    _assert_same(res[1][0], res[0][0], f"{Nx}x{Ny} sp {sp} Nsec {nsec}: block form")
+    assert np.array_equal(res[1][1], res[0][1]), "plane dump differs"
