@@ -277,7 +277,10 @@ int piv_get_stream(const piv_engine *e, void **stream);
  * piv_create (windows per CTA, threads per CTA) and its measured time per launch on
  * the tuning input (0 if not tuned; PIV_AUTOTUNE=0/off/false/no keeps the defaults,
  * PIV_XCORR_VARIANT=v1,v2 fixes them).  The variants compute the same bits, so the
- * choice changes speed only.  A grid on the generic-size kernel reports (1, 256, 0). */
+ * choice changes speed only.  32x32 windows have one more variant after their row-major
+ * ones (index 5): two horizontally adjacent window pairs of two consecutive window rows per
+ * CTA, sharing their overlapping pixel rows' gathers and row transforms, reported as
+ * (4, 128).  A grid on the generic-size kernel reports (1, 256, 0). */
 int piv_xcorr_config(const piv_engine *e, int grid, int *windows_per_cta, int *threads_per_cta, float *tuned_ms);
 
 /* Correlation path of a grid (0 = grid 1, 1 = grid 2).  PIV_XCORR_SIMT: register FFTs in FP32 on the CUDA cores
