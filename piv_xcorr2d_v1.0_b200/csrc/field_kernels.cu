@@ -76,9 +76,11 @@ __device__ __forceinline__ float cell_coord(float v, float st, float sp, float i
 
 // Each thread writes 8 consecutive pixels of one row (two float4 stores).  When the
 // vector spacing and the field origin are multiples of 8 (the `cell8` launches), the 8
-// pixels lie in one cell of the field, so its 8 values are loaded once.
+// pixels lie in one cell of the field, so its 8 values are loaded once.  Bounded to 6
+// blocks per SM (40 registers; the byte gathers want the warps: 88 -> 82 us at the
+// 6600x4400 workload, against no change at 5 blocks and the unbounded 54 registers' 4).
 template <bool CELL8, bool POW2>
-__global__ void __launch_bounds__(256) deform_kernel(const DeformArgs a)
+__global__ void __launch_bounds__(256, 6) deform_kernel(const DeformArgs a)
 {
     const int X0 = (blockIdx.x * blockDim.x + threadIdx.x) * 8;
     const int Y = blockIdx.y;
